@@ -1,0 +1,857 @@
+// The C ABI of include/bhg.h: contexts, device memory, the per-phase calls
+// and the captured whole-step graph.
+#include "bhg.h"
+#include "bhg_kernels.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace bhg;
+
+namespace {
+
+constexpr uint32_t kStackCap = 8192;  // per-warp walk stack (one pop per step beyond it)
+constexpr uint32_t kFatal = kStNonFinite | kStNodeOverflow | kStSpinLimit | kStTooLarge;
+
+enum Ev { kEvStart, kEvSortStart, kEvSortEnd, kEvBuildEnd, kEvMomEnd, kEvWalkStart, kEvWalkEnd, kEvCount };
+
+// Event record that also works inside stream capture (an event-record node).
+inline void rec(cudaEvent_t e, cudaStream_t s) { cudaEventRecordWithFlags(e, s, cudaEventRecordExternal); }
+
+}  // namespace
+
+struct bhg_context {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint64_t budget = 0, allocated = 0;
+  std::string err;
+
+  // current problem
+  size_t n = 0;
+  int nsys = 0;
+  std::vector<SysDev> sys_host;
+  std::vector<SysParam> prm_host;
+  std::vector<Tile> tiles_host;
+  std::vector<std::pair<void*, size_t>> allocs;
+
+  // capacities
+  size_t cap_n = 0, cap_nodes = 0, cap_sys = 0, cap_tiles = 0, cap_stack_warps = 0;
+
+  // device buffers
+  Particle *part = nullptr, *staged = nullptr;
+  double4* pm = nullptr;
+  uint64_t* keys[2] = {nullptr, nullptr};
+  uint32_t* vals[2] = {nullptr, nullptr};
+  uint32_t *hist = nullptr, *offs = nullptr, *sort_lb = nullptr;
+  double* partial = nullptr;
+  Tile* tiles = nullptr;
+  SysDev* sys = nullptr;
+  SysParam* prm = nullptr;
+  Nodes nd{};
+  uint32_t *level_lb = nullptr, *mark = nullptr, *targets = nullptr, *scan_lb = nullptr, *stack = nullptr;
+  double* accel = nullptr;
+  DevState* st = nullptr;
+  DevState* st_host = nullptr;  // pinned
+
+  // phase state
+  bool built = false, moments = false, walked = false;
+  unsigned max_leaf = 16;
+  uint32_t group_size = 256;
+  int quad = 1, precision = 0;
+  bool mask = false;
+
+  // timing
+  cudaEvent_t ev[kEvCount] = {};
+  bool timed_build = false, timed_walk = false;
+
+  // captured whole-step graph
+  cudaGraphExec_t graph = nullptr;
+  std::string graph_key;
+};
+
+namespace {
+
+int fail(bhg_context* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail(c, BHG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int dev_alloc(bhg_context* c, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  if (c->budget && c->allocated + bytes > c->budget)
+    return fail(c, BHG_ENOMEM, "HBM budget exceeded: need " + std::to_string(c->allocated + bytes) + " bytes of " +
+                                   std::to_string(c->budget));
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, BHG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  c->allocated += bytes;
+  c->allocs.push_back({*p, bytes});
+  return BHG_OK;
+}
+
+void dev_free(bhg_context* c, void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < c->allocs.size(); ++i) {
+    if (c->allocs[i].first == p) {
+      c->allocated -= c->allocs[i].second;
+      c->allocs.erase(c->allocs.begin() + (long)i);
+      break;
+    }
+  }
+  cudaFree(p);
+}
+
+template <typename T>
+int grow(bhg_context* c, T** p, size_t count) {
+  dev_free(c, *p);
+  *p = nullptr;
+  return dev_alloc(c, reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+void drop_graph(bhg_context* c) {
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->graph = nullptr;
+  c->graph_key.clear();
+}
+
+// Node slots for n particles: about 0.25 per particle at max_leaf 16 on
+// Plummer spheres, up to ~1.5 at max_leaf 1; grown on overflow.
+size_t node_estimate(size_t n, int nsys, unsigned max_leaf) {
+  double per = max_leaf <= 1 ? 2.2 : max_leaf <= 4 ? 1.2 : max_leaf <= 8 ? 0.7 : 0.45;
+  return std::max<size_t>(1024, (size_t)(per * (double)n) + 64 * (size_t)nsys + 64);
+}
+
+int ensure_nodes(bhg_context* c, size_t need) {
+  if (need <= c->cap_nodes) return BHG_OK;
+  size_t cap = need;
+  drop_graph(c);
+  int r;
+  if ((r = grow(c, &c->nd.begin, cap)) || (r = grow(c, &c->nd.count, cap)) || (r = grow(c, &c->nd.first, cap)) ||
+      (r = grow(c, &c->nd.info, cap)) || (r = grow(c, &c->nd.box, cap)) || (r = grow(c, &c->nd.mom, cap)) ||
+      (r = grow(c, &c->nd.iab, cap * 6)) || (r = grow(c, &c->nd.w, cap)) || (r = grow(c, &c->nd.q45, cap)) ||
+      (r = grow(c, &c->nd.q64, cap * 6)) || (r = grow(c, &c->targets, cap)) ||
+      (r = grow(c, &c->level_lb, cap / 32 + kLevels + 8)))
+    return r;
+  c->nd.cap = (uint32_t)cap;
+  c->cap_nodes = cap;
+  return BHG_OK;
+}
+
+// Particle-sized buffers and the per-system tables for the current problem.
+int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles) {
+  int r;
+  if (n > c->cap_n) {
+    drop_graph(c);
+    dev_free(c, c->accel);
+    c->accel = nullptr;
+    if ((r = grow(c, &c->part, n)) || (r = grow(c, &c->staged, n)) || (r = grow(c, &c->pm, n)) ||
+        (r = grow(c, &c->keys[0], n)) || (r = grow(c, &c->keys[1], n)) || (r = grow(c, &c->vals[0], n)) ||
+        (r = grow(c, &c->vals[1], n)) || (r = grow(c, &c->mark, n)) || (r = grow(c, &c->scan_lb, n / 4096 + 8)))
+      return r;
+    CK(cudaMemsetAsync(c->mark, 0xff, n * sizeof(uint32_t), c->stream));
+    c->cap_n = n;
+  }
+  if ((size_t)nsys > c->cap_sys) {
+    drop_graph(c);
+    if ((r = grow(c, &c->sys, nsys)) || (r = grow(c, &c->prm, nsys)) ||
+        (r = grow(c, &c->hist, (size_t)nsys * kSortPasses * 256)) || (r = grow(c, &c->offs, (size_t)nsys * kSortPasses * 256)))
+      return r;
+    c->cap_sys = nsys;
+  }
+  if (ntiles > c->cap_tiles) {
+    drop_graph(c);
+    if ((r = grow(c, &c->tiles, ntiles)) || (r = grow(c, &c->partial, ntiles * 6)) ||
+        (r = grow(c, &c->sort_lb, ntiles * kSortPasses * 256)))
+      return r;
+    c->cap_tiles = ntiles;
+  }
+  return BHG_OK;
+}
+
+int walk_grid(bhg_context* c) {
+  int per = walk_blocks_per_sm(c->precision, c->quad != 0, c->mask);
+  return c->sms * per;
+}
+
+int ensure_stack(bhg_context* c, int grid) {
+  size_t warps = (size_t)grid * (walk_threads() / 32);
+  if (warps <= c->cap_stack_warps) return BHG_OK;
+  drop_graph(c);
+  int r = grow(c, &c->stack, warps * kStackCap);
+  if (r) return r;
+  c->cap_stack_warps = warps;
+  return BHG_OK;
+}
+
+// Lays out systems and sort tiles for particle counts `counts`.
+int set_problem(bhg_context* c, const uint64_t* counts, size_t nsys) {
+  if (nsys == 0) return fail(c, BHG_EINVAL, "no systems");
+  size_t n = 0, ntiles = 0;
+  for (size_t s = 0; s < nsys; ++s) {
+    if (counts[s] == 0) return fail(c, BHG_EINVAL, "system " + std::to_string(s) + " has no particles");
+    n += counts[s];
+    ntiles += (counts[s] + kTile - 1) / kTile;
+  }
+  if (n >= (1ull << 30)) return fail(c, BHG_EINVAL, "more than 2^30 - 1 particles");
+  if (nsys > 65535) return fail(c, BHG_EINVAL, "more than 65535 systems");
+  int r = ensure_particles(c, n, (int)nsys, ntiles);
+  if (r) return r;
+  c->sys_host.assign(nsys, SysDev{});
+  c->tiles_host.clear();
+  uint32_t begin = 0;
+  for (size_t s = 0; s < nsys; ++s) {
+    SysDev& d = c->sys_host[s];
+    d.begin = begin;
+    d.n = (uint32_t)counts[s];
+    d.root = (uint32_t)s;
+    d.tile_begin = (uint32_t)c->tiles_host.size();
+    for (uint32_t o = 0; o < d.n; o += kTile)
+      c->tiles_host.push_back(Tile{(uint32_t)s, begin + o, std::min<uint32_t>(kTile, d.n - o), d.tile_begin});
+    d.tile_count = (uint32_t)c->tiles_host.size() - d.tile_begin;
+    begin += d.n;
+  }
+  if (c->n != n || c->nsys != (int)nsys) drop_graph(c);
+  c->n = n;
+  c->nsys = (int)nsys;
+  c->prm_host.assign(nsys, SysParam{0.25, 0.0, 1.0, 0.0, 0.0, {0, 0, 0}});
+  CK(cudaMemcpyAsync(c->sys, c->sys_host.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->tiles, c->tiles_host.data(), c->tiles_host.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemsetAsync(c->st, 0, sizeof(DevState), c->stream));
+  c->built = c->moments = c->walked = false;
+  return BHG_OK;
+}
+
+// ---- enqueue the phases (no host synchronisation) ---------------------------
+
+void enq_build(bhg_context* c, bool timed) {
+  cudaStream_t s = c->stream;
+  const int nt = (int)c->tiles_host.size();
+  if (timed) rec(c->ev[kEvStart], s);
+  cudaMemsetAsync(reinterpret_cast<char*>(c->st) + kBuildResetOffset, 0, sizeof(DevState) - kBuildResetOffset, s);
+  cudaMemsetAsync(c->hist, 0, (size_t)c->nsys * kSortPasses * 256 * sizeof(uint32_t), s);
+  cudaMemsetAsync(c->sort_lb, 0, (size_t)nt * kSortPasses * 256 * sizeof(uint32_t), s);
+  cudaMemsetAsync(c->level_lb, 0, (c->cap_nodes / 32 + kLevels + 8) * sizeof(uint32_t), s);
+  launch_bounds_domain(c->part, c->tiles, nt, c->sys, c->nsys, c->partial, c->st, s);
+  launch_keys(c->part, c->tiles, nt, c->sys, c->nsys, c->keys[0], c->hist, c->offs, s);
+  if (timed) rec(c->ev[kEvSortStart], s);
+  for (int p = 0; p < kSortPasses; ++p)
+    launch_sort_pass(c->keys[p & 1], c->vals[p & 1], c->keys[(p + 1) & 1], c->vals[(p + 1) & 1], p, c->tiles, nt,
+                     c->offs, c->sort_lb + (size_t)p * nt * 256, c->st, s);
+  if (timed) rec(c->ev[kEvSortEnd], s);
+  // kSortPasses is even: sorted keys and the permutation are back in [0]
+  launch_gather(c->part, c->vals[0], (uint32_t)c->n, c->staged, c->pm, c->sms, s);
+  launch_topology(c->sys, c->nsys, c->nd, c->keys[0], c->max_leaf, c->level_lb, c->st, c->sms, s);
+  if (timed) rec(c->ev[kEvBuildEnd], s);
+}
+
+void enq_moments(bhg_context* c, bool timed) {
+  launch_moments(c->nd, c->pm, c->st, c->sms, c->stream);
+  if (timed) rec(c->ev[kEvMomEnd], c->stream);
+}
+
+void enq_walk(bhg_context* c, uint32_t target_size, bool timed, bool want_accel) {
+  cudaStream_t s = c->stream;
+  cudaMemsetAsync(reinterpret_cast<char*>(c->st) + kWalkResetOffset, 0, sizeof(DevState) - kWalkResetOffset, s);
+  cudaMemsetAsync(c->scan_lb, 0, (c->n / 4096 + 8) * sizeof(uint32_t), s);
+  const uint32_t gs = c->group_size == 0 ? 0u : c->group_size;
+  const uint32_t lim = std::min(target_size, gs);
+  launch_targets(c->nd, lim, (uint32_t)c->n, c->mark, c->targets, c->scan_lb, c->st, c->sms, s);
+  WalkArgs a;
+  a.w = c->nd.w;
+  a.q45 = c->nd.q45;
+  a.q64 = c->nd.q64;
+  a.mom = c->nd.mom;
+  a.nbegin = c->nd.begin;
+  a.ncount = c->nd.count;
+  a.pm = c->pm;
+  a.targets = c->targets;
+  a.sys = c->sys;
+  a.prm = c->prm;
+  a.nsys = c->nsys;
+  a.staged = c->staged;
+  a.out = c->part;
+  a.accel = want_accel ? c->accel : nullptr;
+  a.stack = c->stack;
+  a.stack_cap = kStackCap;
+  a.st = c->st;
+  if (timed) rec(c->ev[kEvWalkStart], s);
+  launch_walk(a, c->precision, c->quad != 0, c->mask, walk_grid(c), s);
+  if (timed) rec(c->ev[kEvWalkEnd], s);
+  launch_eval_done(c->st, s);
+}
+
+int push_params(bhg_context* c) {
+  CK(cudaMemcpyAsync(c->prm, c->prm_host.data(), c->prm_host.size() * sizeof(SysParam), cudaMemcpyHostToDevice,
+                     c->stream));
+  return BHG_OK;
+}
+
+int read_state(bhg_context* c) {
+  CK(cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BHG_OK;
+}
+
+std::string status_text(uint32_t s) {
+  std::string t;
+  if (s & kStNonFinite) t += " non-finite particle coordinate;";
+  if (s & kStNodeOverflow) t += " octree larger than its node slots;";
+  if (s & kStSpinLimit) t += " a bounded wait in a sort/scan kernel gave up;";
+  if (s & kStTooLarge) t += " a count exceeded 30 bits;";
+  return t;
+}
+
+// After a synchronising read of the state: map sticky device errors to codes.
+int check_status(bhg_context* c) {
+  const uint32_t s = c->st_host->status;
+  if (s == 0) return BHG_OK;
+  if (s & kStNonFinite) return fail(c, BHG_ENONFINITE, "particle coordinates are not finite:" + status_text(s));
+  return fail(c, BHG_EDEVICE, "device reported:" + status_text(s));
+}
+
+int clear_status(bhg_context* c) {
+  CK(cudaMemsetAsync(c->st, 0, sizeof(uint32_t), c->stream));
+  return BHG_OK;
+}
+
+int set_force_params(bhg_context* c, const bhg_force_params* fp, double kick, double drift, bool keep_per_system) {
+  if (!fp) return fail(c, BHG_EINVAL, "null force params");
+  if (!(fp->theta >= 0.0) || !(fp->eps2 >= 0.0) || !std::isfinite(fp->G))
+    return fail(c, BHG_EINVAL, "theta and eps2 must be >= 0, G finite");
+  if (fp->precision != BHG_PRECISION_SPLIT && fp->precision != BHG_PRECISION_FP64)
+    return fail(c, BHG_EINVAL, "unknown precision");
+  const int newq = fp->use_quadrupole ? 1 : 0;
+  const bool newmask = !(fp->eps2 > 0.0);
+  c->quad = newq;
+  c->precision = fp->precision;
+  c->mask = newmask;
+  for (auto& p : c->prm_host) {
+    if (!keep_per_system) {
+      p.theta2 = fp->theta * fp->theta;
+      p.eps2 = fp->eps2;
+      p.kick_dt = kick;
+      p.drift_dt = drift;
+    }
+    p.G = fp->G;
+  }
+  return BHG_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+
+extern "C" {
+
+int bhg_create(bhg_context** out, const bhg_config* cfg) {
+  if (!out) return BHG_EINVAL;
+  *out = nullptr;
+  auto* c = new (std::nothrow) bhg_context;
+  if (!c) return BHG_ENOMEM;
+  c->device = cfg ? cfg->device : 0;
+  c->budget = cfg ? cfg->hbm_budget : 0;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) {
+    delete c;
+    cudaGetLastError();
+    return BHG_ECUDA;
+  }
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return BHG_ECUDA;
+  }
+  c->own_stream = true;
+  for (auto& ev : c->ev) cudaEventCreate(&ev);
+  set_build_attributes();
+  if (dev_alloc(c, reinterpret_cast<void**>(&c->st), sizeof(DevState)) ||
+      cudaMallocHost(&c->st_host, sizeof(DevState)) != cudaSuccess) {
+    bhg_destroy(c);
+    return BHG_ENOMEM;
+  }
+  cudaMemsetAsync(c->st, 0, sizeof(DevState), c->stream);
+  *out = c;
+  return BHG_OK;
+}
+
+int bhg_destroy(bhg_context* c) {
+  if (!c) return BHG_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graph(c);
+  for (auto& a : c->allocs) cudaFree(a.first);
+  c->allocs.clear();
+  if (c->st_host) cudaFreeHost(c->st_host);
+  for (auto& ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return BHG_OK;
+}
+
+const char* bhg_last_error(const bhg_context* c) { return c ? c->err.c_str() : "null context"; }
+
+int bhg_set_stream(bhg_context* c, void* s) {
+  if (!c) return BHG_EINVAL;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graph(c);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  if (s) {
+    c->stream = static_cast<cudaStream_t>(s);
+    c->own_stream = false;
+  } else {
+    cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    c->own_stream = true;
+  }
+  return BHG_OK;
+}
+
+static int upload_impl(bhg_context* c, const void* src, const uint64_t* counts, size_t nsys, cudaMemcpyKind kind) {
+  if (!c || (!src && counts && counts[0])) return fail(c, BHG_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  int r = set_problem(c, counts, nsys);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->part, src, c->n * sizeof(Particle), kind, c->stream));
+  return BHG_OK;
+}
+
+int bhg_upload(bhg_context* c, const bh_particle64* p, size_t n) {
+  uint64_t cnt = n;
+  return upload_impl(c, p, &cnt, 1, cudaMemcpyHostToDevice);
+}
+
+int bhg_upload_device(bhg_context* c, const void* p, size_t n) {
+  uint64_t cnt = n;
+  return upload_impl(c, p, &cnt, 1, cudaMemcpyDeviceToDevice);
+}
+
+int bhg_upload_systems(bhg_context* c, const bh_particle64* p, const uint64_t* counts, size_t nsys) {
+  if (!counts) return fail(c, BHG_EINVAL, "null counts");
+  return upload_impl(c, p, counts, nsys, cudaMemcpyHostToDevice);
+}
+
+int bhg_download(bhg_context* c, bh_particle64* out) {
+  if (!c || !out) return fail(c, BHG_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  CK(cudaMemcpyAsync(out, c->part, c->n * sizeof(Particle), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BHG_OK;
+}
+
+int bhg_download_device(bhg_context* c, void* out) {
+  if (!c || !out) return fail(c, BHG_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  CK(cudaMemcpyAsync(out, c->part, c->n * sizeof(Particle), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BHG_OK;
+}
+
+size_t bhg_num_particles(const bhg_context* c) { return c ? c->n : 0; }
+
+int bhg_build_tree(bhg_context* c, unsigned max_leaf, uint32_t group_size) {
+  if (!c) return BHG_EINVAL;
+  if (c->n == 0) return fail(c, BHG_ESTATE, "no particles uploaded");
+  if (max_leaf == 0) return fail(c, BHG_EINVAL, "max_leaf must be >= 1");
+  cudaSetDevice(c->device);
+  c->max_leaf = max_leaf;
+  c->group_size = group_size;
+  int r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf));
+  if (r) return r;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    enq_build(c, true);
+    c->timed_build = true;
+    if ((r = read_state(c))) return r;
+    if (c->st_host->status & kStNodeOverflow) {
+      size_t need = (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64;
+      if ((r = clear_status(c)) || (r = ensure_nodes(c, need))) return r;
+      continue;
+    }
+    if ((r = check_status(c))) {
+      clear_status(c);
+      return r;
+    }
+    c->built = true;
+    c->moments = c->walked = false;
+    return BHG_OK;
+  }
+  return fail(c, BHG_EDEVICE, "octree kept outgrowing its node slots");
+}
+
+int bhg_compute_multipoles(bhg_context* c) {
+  if (!c) return BHG_EINVAL;
+  if (!c->built) return fail(c, BHG_ESTATE, "build the tree first");
+  cudaSetDevice(c->device);
+  rec(c->ev[kEvBuildEnd], c->stream);
+  enq_moments(c, true);
+  c->moments = true;
+  return BHG_OK;
+}
+
+int bhg_walk_forces(bhg_context* c, const bhg_force_params* fp, uint32_t target_size, double kick_dt,
+                    double drift_dt, double* accel_out, uint64_t* missing) {
+  if (!c) return BHG_EINVAL;
+  if (!c->moments) return fail(c, BHG_ESTATE, "compute the multipoles first");
+  cudaSetDevice(c->device);
+  int r = set_force_params(c, fp, kick_dt, drift_dt, false);
+  if (r) return r;
+  if (!c->accel && (r = grow(c, &c->accel, c->cap_n * 3))) return r;
+  if ((r = ensure_stack(c, walk_grid(c))) || (r = push_params(c))) return r;
+  enq_walk(c, target_size, true, true);
+  c->timed_walk = true;
+  c->walked = true;
+  c->moments = false;  // the state moved: the next walk needs a new build
+  c->built = false;
+  if (missing) *missing = 0;
+  if ((r = read_state(c))) return r;
+  if ((r = check_status(c))) {
+    clear_status(c);
+    return r;
+  }
+  if (accel_out) {
+    CK(cudaMemcpyAsync(accel_out, c->accel, c->n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return BHG_OK;
+}
+
+int bhg_integrate(bhg_context* c, double kick_dt, double drift_dt) {
+  if (!c) return BHG_EINVAL;
+  if (!c->walked || !c->accel) return fail(c, BHG_ESTATE, "walk forces first");
+  cudaSetDevice(c->device);
+  for (auto& p : c->prm_host) {
+    p.kick_dt = kick_dt;
+    p.drift_dt = drift_dt;
+  }
+  int r = push_params(c);
+  if (r) return r;
+  launch_integrate(c->part, c->accel, (uint32_t)c->n, c->sys, c->prm, c->nsys, c->sms, c->stream);
+  CK(cudaGetLastError());
+  return BHG_OK;
+}
+
+int bhg_set_system_params(bhg_context* c, const double* theta, const double* eps2, const double* kick_dt,
+                          const double* drift_dt) {
+  if (!c) return BHG_EINVAL;
+  for (int s = 0; s < c->nsys; ++s) {
+    SysParam& p = c->prm_host[s];
+    if (theta) p.theta2 = theta[s] * theta[s];
+    if (eps2) p.eps2 = eps2[s];
+    if (kick_dt) p.kick_dt = kick_dt[s];
+    if (drift_dt) p.drift_dt = drift_dt[s];
+  }
+  return BHG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One whole evaluation (build + multipoles + walk), replayed from a graph.
+int enq_step(bhg_context* c, uint32_t target_size, bool timed) {
+  char key[160];
+  snprintf(key, sizeof key, "%zu/%d/%zu/%u/%u/%u/%d/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->max_leaf,
+           c->group_size, target_size, c->precision, c->quad, (int)c->mask, (int)timed);
+  if (!c->graph || c->graph_key != key) {
+    drop_graph(c);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enq_build(c, timed);
+    enq_moments(c, timed);
+    enq_walk(c, target_size, timed, false);
+    CK(cudaStreamEndCapture(c->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      c->graph = nullptr;
+      return fail(c, BHG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    c->graph_key = key;
+  }
+  CK(cudaGraphLaunch(c->graph, c->stream));
+  return BHG_OK;
+}
+
+int prepare_step(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
+                 double kick, double drift, bool keep) {
+  if (c->n == 0) return fail(c, BHG_ESTATE, "no particles uploaded");
+  if (max_leaf == 0) return fail(c, BHG_EINVAL, "max_leaf must be >= 1");
+  cudaSetDevice(c->device);
+  int r = set_force_params(c, fp, kick, drift, keep);
+  if (r) return r;
+  if (c->max_leaf != max_leaf || c->group_size != group_size) drop_graph(c);
+  c->max_leaf = max_leaf;
+  c->group_size = group_size;
+  if ((r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf))) || (r = ensure_stack(c, walk_grid(c))))
+    return r;
+  return BHG_OK;
+}
+
+// Runs evaluations i0 .. i1-1 of a schedule given by kick/drift per
+// evaluation; on a node overflow grows the slots and resumes from the
+// evaluation that failed (its walk was skipped, so the state is intact).
+int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<double, double>>& kd, bool keep) {
+  size_t next = 0;
+  for (int attempt = 0; attempt < 6; ++attempt) {
+    int r;
+    if ((r = read_state(c))) return r;
+    const uint32_t base = c->st_host->evals_ok;
+    for (size_t i = next; i < kd.size(); ++i) {
+      if (!keep) {
+        for (auto& p : c->prm_host) {
+          p.kick_dt = kd[i].first;
+          p.drift_dt = kd[i].second;
+        }
+      }
+      if ((r = push_params(c)) || (r = enq_step(c, target_size, true))) return r;
+    }
+    if ((r = read_state(c))) return r;
+    const uint32_t done = c->st_host->evals_ok - base;
+    if (c->st_host->status == 0) {
+      c->timed_build = c->timed_walk = true;
+      c->walked = true;
+      c->built = c->moments = false;
+      return BHG_OK;
+    }
+    if (c->st_host->status & kStNodeOverflow) {
+      next += done;
+      size_t need = (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64;
+      if ((r = clear_status(c)) || (r = ensure_nodes(c, need)) || (r = ensure_stack(c, walk_grid(c)))) return r;
+      continue;
+    }
+    r = check_status(c);
+    clear_status(c);
+    return r;
+  }
+  return fail(c, BHG_EDEVICE, "octree kept outgrowing its node slots");
+}
+
+}  // namespace
+
+extern "C" {
+
+int bhg_step(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
+             uint32_t target_size, double kick_dt, double drift_dt) {
+  if (!c) return BHG_EINVAL;
+  int r = prepare_step(c, fp, max_leaf, group_size, kick_dt, drift_dt, false);
+  if (r) return r;
+  return run_evals(c, target_size, {{kick_dt, drift_dt}}, false);
+}
+
+int bhg_step_systems(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
+                     uint32_t target_size) {
+  if (!c) return BHG_EINVAL;
+  int r = prepare_step(c, fp, max_leaf, group_size, 0.0, 0.0, true);
+  if (r) return r;
+  return run_evals(c, target_size, {{0.0, 0.0}}, true);
+}
+
+int bhg_run_schedule(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
+                     uint32_t target_size, double dt, int steps) {
+  if (!c) return BHG_EINVAL;
+  if (steps < 1) return fail(c, BHG_EINVAL, "steps must be >= 1");
+  int r = prepare_step(c, fp, max_leaf, group_size, dt / 2.0, dt, false);
+  if (r) return r;
+  std::vector<std::pair<double, double>> kd;
+  kd.push_back({dt / 2.0, dt});                                 // main.cc:206-208
+  for (int s = 1; s < steps; ++s) kd.push_back({dt, dt});       // main.cc:219-222
+  kd.push_back({dt / 2.0, 0.0});                                // main.cc:240-242
+  return run_evals(c, target_size, kd, false);
+}
+
+int bhg_get_stats(bhg_context* c, bhg_stats* out) {
+  if (!c || !out) return BHG_EINVAL;
+  cudaSetDevice(c->device);
+  int r = read_state(c);
+  if (r) return r;
+  std::memset(out, 0, sizeof *out);
+  float ms = 0.f;
+  auto el = [&](int a, int b) -> double {
+    if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) {
+      cudaGetLastError();
+      return -1.0;
+    }
+    return ms;
+  };
+  if (c->timed_build) {
+    out->build_ms = el(kEvStart, kEvBuildEnd);
+    out->sort_ms = el(kEvSortStart, kEvSortEnd);
+    out->multipole_ms = el(kEvBuildEnd, kEvMomEnd);
+  }
+  if (c->timed_walk) out->walk_ms = el(kEvWalkStart, kEvWalkEnd);
+  out->pp = c->st_host->pp;
+  out->pc = c->st_host->pc;
+  out->nodes = c->st_host->n_nodes;
+  out->targets = c->st_host->n_targets;
+  out->depth = c->st_host->max_depth;
+  out->sort_passes = kSortPasses;
+  return BHG_OK;
+}
+
+int bhg_device_status(bhg_context* c, uint32_t* status) {
+  if (!c || !status) return BHG_EINVAL;
+  cudaSetDevice(c->device);
+  int r = read_state(c);
+  if (r) return r;
+  *status = c->st_host->status;
+  return BHG_OK;
+}
+
+int bhg_debug_export(bhg_context* c, int what, void* out, size_t bytes, size_t* written) {
+  if (!c) return BHG_EINVAL;
+  cudaSetDevice(c->device);
+  int r = read_state(c);
+  if (r) return r;
+  const size_t nn = std::min<size_t>(c->st_host->n_nodes, c->cap_nodes);
+  std::vector<char> buf;
+  auto get = [&](const void* src, size_t b, size_t at) -> int {
+    CK(cudaMemcpy(buf.data() + at, src, b, cudaMemcpyDeviceToHost));
+    return BHG_OK;
+  };
+  switch (what) {
+    case BHG_EXPORT_KEYS:
+      buf.resize(c->n * 8);
+      if ((r = get(c->keys[0], buf.size(), 0))) return r;
+      break;
+    case BHG_EXPORT_PERM:
+      buf.resize(c->n * 4);
+      if ((r = get(c->vals[0], buf.size(), 0))) return r;
+      break;
+    case BHG_EXPORT_NODES_U32: {
+      buf.resize(nn * 24);
+      if ((r = get(c->nd.begin, nn * 4, 0)) || (r = get(c->nd.count, nn * 4, nn * 4)) ||
+          (r = get(c->nd.first, nn * 4, nn * 8)))
+        return r;
+      std::vector<uint32_t> info(nn);
+      CK(cudaMemcpy(info.data(), c->nd.info, nn * 4, cudaMemcpyDeviceToHost));
+      uint32_t* u = reinterpret_cast<uint32_t*>(buf.data());
+      for (size_t i = 0; i < nn; ++i) {
+        u[3 * nn + i] = info_nchild(info[i]);
+        u[4 * nn + i] = info_leaf(info[i]) ? 1u : 0u;
+        u[5 * nn + i] = info_depth(info[i]);
+        if (u[4 * nn + i]) u[2 * nn + i] = 0;  // first_child of a leaf
+      }
+      break;
+    }
+    case BHG_EXPORT_NODES_F64: {
+      buf.resize(nn * 14 * 8);
+      std::vector<double4> box(nn), mom(nn);
+      std::vector<double> iab(nn * 6);
+      CK(cudaMemcpy(box.data(), c->nd.box, nn * sizeof(double4), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(mom.data(), c->nd.mom, nn * sizeof(double4), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(iab.data(), c->nd.iab, nn * 48, cudaMemcpyDeviceToHost));
+      double* d = reinterpret_cast<double*>(buf.data());
+      for (size_t i = 0; i < nn; ++i) {
+        double* o = d + 14 * i;
+        o[0] = box[i].x, o[1] = box[i].y, o[2] = box[i].z, o[3] = box[i].w;
+        o[4] = mom[i].w, o[5] = mom[i].x, o[6] = mom[i].y, o[7] = mom[i].z;
+        for (int k = 0; k < 6; ++k) o[8 + k] = iab[6 * i + k];
+      }
+      break;
+    }
+    case BHG_EXPORT_DOMAINS: {
+      std::vector<SysDev> sd(c->nsys);
+      CK(cudaMemcpy(sd.data(), c->sys, c->nsys * sizeof(SysDev), cudaMemcpyDeviceToHost));
+      buf.resize((size_t)c->nsys * 32);
+      double* d = reinterpret_cast<double*>(buf.data());
+      for (int s = 0; s < c->nsys; ++s) d[4 * s] = sd[s].cx, d[4 * s + 1] = sd[s].cy, d[4 * s + 2] = sd[s].cz, d[4 * s + 3] = sd[s].hw;
+      break;
+    }
+    case BHG_EXPORT_TARGETS:
+      buf.resize((size_t)c->st_host->n_targets * 4);
+      if ((r = get(c->targets, buf.size(), 0))) return r;
+      break;
+    case BHG_EXPORT_ACCEL:
+      if (!c->accel) return fail(c, BHG_ESTATE, "no accelerations stored (bhg_walk_forces stores them)");
+      buf.resize(c->n * 24);
+      if ((r = get(c->accel, buf.size(), 0))) return r;
+      break;
+    default:
+      return fail(c, BHG_EINVAL, "unknown export");
+  }
+  if (written) *written = buf.size();
+  if (out) {
+    if (bytes < buf.size()) return fail(c, BHG_EINVAL, "export buffer too small");
+    std::memcpy(out, buf.data(), buf.size());
+  }
+  return BHG_OK;
+}
+
+int bhg_direct_sum(bhg_context* c, int sys, const uint32_t* idx, size_t ns, double eps2, double G, double* out) {
+  if (!c || !idx || !out) return fail(c, BHG_EINVAL, "null argument");
+  if (sys < 0 || sys >= c->nsys) return fail(c, BHG_EINVAL, "no such system");
+  cudaSetDevice(c->device);
+  const SysDev& d = c->sys_host[sys];
+  for (size_t k = 0; k < ns; ++k)
+    if (idx[k] >= d.n) return fail(c, BHG_EINVAL, "sample index out of range");
+  // positions of the current state (output order) into pm
+  int r;
+  uint32_t* didx = nullptr;
+  double* dout = nullptr;
+  double4* dpm = nullptr;
+  if ((r = dev_alloc(c, (void**)&didx, ns * 4)) || (r = dev_alloc(c, (void**)&dout, ns * 24)) ||
+      (r = dev_alloc(c, (void**)&dpm, (size_t)d.n * sizeof(double4)))) {
+    dev_free(c, didx), dev_free(c, dout), dev_free(c, dpm);
+    return r;
+  }
+  std::vector<Particle> hp(d.n);
+  cudaMemcpyAsync(hp.data(), c->part + d.begin, (size_t)d.n * sizeof(Particle), cudaMemcpyDeviceToHost, c->stream);
+  cudaStreamSynchronize(c->stream);
+  std::vector<double4> h4(d.n);
+  for (uint32_t i = 0; i < d.n; ++i) h4[i] = make_double4(hp[i].pos[0], hp[i].pos[1], hp[i].pos[2], hp[i].mass);
+  cudaMemcpyAsync(dpm, h4.data(), (size_t)d.n * sizeof(double4), cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(didx, idx, ns * 4, cudaMemcpyHostToDevice, c->stream);
+  launch_direct(dpm, 0, d.n, didx, (uint32_t)ns, eps2, G, dout, c->stream);
+  cudaError_t e = cudaMemcpyAsync(out, dout, ns * 24, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  dev_free(c, didx), dev_free(c, dout), dev_free(c, dpm);
+  if (e != cudaSuccess) return fail(c, BHG_ECUDA, cudaGetErrorString(e));
+  return BHG_OK;
+}
+
+int bhg_energy(bhg_context* c, int sys, double G, double* kinetic, double* potential) {
+  if (!c) return BHG_EINVAL;
+  if (sys < 0 || sys >= c->nsys) return fail(c, BHG_EINVAL, "no such system");
+  cudaSetDevice(c->device);
+  const SysDev& d = c->sys_host[sys];
+  const uint32_t blocks = (d.n + 255) / 256;
+  double* dout = nullptr;
+  int r = dev_alloc(c, (void**)&dout, (size_t)blocks * 16);
+  if (r) return r;
+  launch_energy(c->part, d.begin, d.n, G, dout, c->sms, c->stream);
+  std::vector<double> h((size_t)blocks * 2);
+  cudaError_t e = cudaMemcpyAsync(h.data(), dout, h.size() * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  dev_free(c, dout);
+  if (e != cudaSuccess) return fail(c, BHG_ECUDA, cudaGetErrorString(e));
+  double ek = 0, ep = 0;
+  for (uint32_t b = 0; b < blocks; ++b) ek += h[2 * b], ep += h[2 * b + 1];
+  if (kinetic) *kinetic = ek;
+  if (potential) *potential = ep;
+  return BHG_OK;
+}
+
+int bhg_measure_fp32_peak(int device, double* tflops) {
+  if (!tflops) return BHG_EINVAL;
+  *tflops = measure_fp32_peak(device);
+  return *tflops > 0 ? BHG_OK : BHG_ECUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// Host-side launchers of the build and walk kernels (bhg_build.cu,
+// bhg_walk.cu), used by the context code in bhg_api.cu.
+#pragma once
+
+#include "bhg_internal.cuh"
+
+namespace bhg {
+
+void set_build_attributes();
+void launch_bounds_domain(const Particle* p, const Tile* tiles, int ntiles, SysDev* sys, int nsys, double* partial,
+                          DevState* st, cudaStream_t s);
+void launch_keys(const Particle* p, const Tile* tiles, int ntiles, const SysDev* sys, int nsys, uint64_t* keys,
+                 uint32_t* hist, uint32_t* offs, cudaStream_t s);
+void launch_sort_pass(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout, int pass,
+                      const Tile* tiles, int ntiles, const uint32_t* offs, uint32_t* lookback, DevState* st,
+                      cudaStream_t s);
+void launch_gather(const Particle* p, const uint32_t* perm, uint32_t n, Particle* staged, double4* pm, int sms,
+                   cudaStream_t s);
+void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_t* keys, unsigned max_leaf,
+                     uint32_t* lookback, DevState* st, int sms, cudaStream_t s);
+// Walk targets: the topmost nodes that are leaves or hold at most `lim`
+// particles.  The reference visits each group root - the topmost nodes with
+// at most group_size particles, or leaves (is_group_root,
+// flat_tree.h:190-192) - and descends to the first node that is a leaf or
+// holds at most target_size particles (grouped_ttg.h:253); on every
+// root-to-leaf path that is the deeper of the two cuts, i.e. the first node
+// with count <= min(target_size, group_size).  group_size 0 (the per-node
+// pass) and target_size 0 both give the leaves.
+void launch_targets(const Nodes& nd, uint32_t lim, uint32_t n, uint32_t* mark, uint32_t* targets,
+                    uint32_t* lookback, DevState* st, int sms, cudaStream_t s);
+void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, cudaStream_t s);
+
+struct WalkArgs {
+  const WNode* w;
+  const float2* q45;
+  const double* q64;
+  const double4* mom;  // FP64 centre of mass + mass (the FP64 walk)
+  const uint32_t* nbegin;
+  const uint32_t* ncount;
+  const double4* pm;
+  const uint32_t* targets;
+  const SysDev* sys;
+  const SysParam* prm;
+  int nsys;
+  const Particle* staged;  // Morton-ordered input of this step
+  Particle* out;           // kicked/drifted particles (the state)
+  double* accel;           // optional: G*a, 3 per particle
+  uint32_t* stack;         // per-warp traversal stacks
+  uint32_t stack_cap;
+  DevState* st;
+};
+
+// Walks every target and kicks/drifts its particles.  precision:
+// 0 = split (FP32 offsets and FP32 interactions, FP64 sums), 1 = FP64.
+void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s);
+int walk_blocks_per_sm(int precision, bool quad, bool mask);
+int walk_threads();
+
+void launch_integrate(Particle* p, const double* accel, uint32_t n, const SysDev* sys, const SysParam* prm, int nsys,
+                      int sms, cudaStream_t s);
+// Counts a finished evaluation when no error bit is set.
+void launch_eval_done(DevState* st, cudaStream_t s);
+void launch_direct(const double4* pm, uint32_t begin, uint32_t n, const uint32_t* idx, uint32_t ns, double eps2,
+                   double G, double* out, cudaStream_t s);
+void launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int sms, cudaStream_t s);
+double measure_fp32_peak(int device);
+
+}  // namespace bhg

@@ -1,0 +1,192 @@
+"""GPU parity of every phase against the oracle (oracle/bh_oracle.c), through
+the C ABI.  Integer results (keys, order, topology) and the FP64 build
+(domain, cell geometry, multipoles) must be bit-identical; forces within
+the stated tolerances:
+
+  FP64 walk   vs oracle walk: global relative error <= 1e-12
+  split walk  vs oracle walk: global relative error <= 1e-5 (north-star gate)
+  theta = 0   vs direct sum:  <= 1e-8 (FP64) / 1e-5 (split), as
+              test_bh_vs_bruteforce.cc:55-76 requires of the reference
+"""
+import numpy as np
+import pytest
+
+import bhg
+from helpers import cube, rel_error
+from oracle import Params, soa
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # name, particles, max_leaf, group_size, target_size, theta, eps2
+    ("cube2000_leaf8", lambda: cube(2000, 4), 8, 64, 0, 0.5, 1e-6),
+    ("cube20000_leaf16", lambda: cube(20000, 5), 16, 64, 0, 0.5, 1e-6),
+    ("plummer32k_leaf16", lambda: bhg.plummer(32768, 1)[0], 16, 256, 16, 0.5, 1e-4),
+    ("cube2000_leaf1_ts32", lambda: cube(2000, 6), 1, 64, 32, 0.5, 1e-6),
+    ("cube3000_leaf4_gs1M", lambda: cube(3000, 7), 4, 1 << 20, 0, 0.6, 1e-6),
+]
+
+
+def _oracle_build(oracle, parts, max_leaf):
+    dom, bad = oracle.domain(parts)
+    assert bad == 0
+    keys = oracle.keys(parts, dom)
+    perm, sk = oracle.sort(keys)
+    mp = parts[perm]
+    t = oracle.build(sk, [0], [len(parts)], dom[None], max_leaf, soa(mp))
+    return dom, sk, perm, mp, t
+
+
+@pytest.mark.parametrize("name,make,max_leaf,gs,ts,theta,eps2", CASES, ids=[c[0] for c in CASES])
+def test_build_bit_exact(gpu, oracle, name, make, max_leaf, gs, ts, theta, eps2):
+    parts = make()
+    dom, sk, perm, mp, t = _oracle_build(oracle, parts, max_leaf)
+    gpu.upload(parts)
+    gpu.build_tree(max_leaf, gs)
+    gpu.compute_multipoles()
+    assert np.array_equal(gpu.export(bhg.EXPORT_DOMAINS)[0], dom), "domain differs"
+    assert np.array_equal(gpu.export(bhg.EXPORT_KEYS), sk), "sorted keys differ"
+    assert np.array_equal(gpu.export(bhg.EXPORT_PERM), perm), "sort permutation differs"
+    g = gpu.tree()
+    n = t["n"]
+    assert g["n"] == n, f"node count {g['n']} != {n}"
+    for k in ("begin", "count", "first_child", "nchild", "leaf", "depth"):
+        assert np.array_equal(g[k], t[k][:n]), f"node {k} differs"
+    for k in ("center", "hw", "mass", "com", "iab"):
+        assert np.array_equal(g[k], np.asarray(t[k][:n])), f"node {k} not bit-identical"
+
+
+@pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-12), (bhg.PRECISION_SPLIT, 1e-5)])
+@pytest.mark.parametrize("name,make,max_leaf,gs,ts,theta,eps2", CASES, ids=[c[0] for c in CASES])
+def test_walk_matches_oracle(gpu, oracle, name, make, max_leaf, gs, ts, theta, eps2, precision, tol):
+    parts = make()
+    for quad in (True, False):
+        dom, sk, perm, mp, t = _oracle_build(oracle, parts, max_leaf)
+        tg = oracle.targets(t, ts, gs)
+        racc, counts = oracle.walk(t, tg, soa(mp), [Params(theta, eps2, 1.0, int(quad))] * len(tg))
+        gpu.upload(parts)
+        gpu.build_tree(max_leaf, gs)
+        gpu.compute_multipoles()
+        acc = gpu.walk_forces(bhg.Context.params(theta, eps2, 1.0, quad, precision), ts)
+        assert np.array_equal(gpu.export(bhg.EXPORT_TARGETS), tg), "targets differ"
+        st = gpu.stats()
+        assert (st["pp"], st["pc"]) == (int(counts[0]), int(counts[1])), "interaction counts differ"
+        err = rel_error(acc, racc)
+        assert err <= tol, f"quad={quad} relative error {err:.3e} > {tol}"
+        out = gpu.download()
+        assert np.array_equal(out["id"], mp["id"]), "output not in Morton order"
+
+
+@pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-8), (bhg.PRECISION_SPLIT, 1e-5)])
+def test_theta0_is_direct_sum(gpu, oracle, precision, tol):
+    # test_bh_vs_bruteforce.cc:55-76: theta = 0 degenerates into brute force
+    parts = cube(200, 1)
+    gpu.upload(parts)
+    gpu.build_tree(4, 16)
+    gpu.compute_multipoles()
+    acc = gpu.walk_forces(bhg.Context.params(0.0, 1e-6, 1.0, True, precision), 0)
+    out = gpu.download()
+    ref = oracle.direct(soa(out), np.arange(len(out)), 1e-6)
+    assert rel_error(acc, ref) <= tol
+
+
+def test_no_softening_masks_self(gpu, oracle):
+    # eps = 0: r^2 == 0 entries masked (accumulate_list Mask, grouped_ttg.h:117-123)
+    parts = cube(3000, 9)
+    parts["pos"][7] = parts["pos"][8]  # a duplicate position
+    gpu.upload(parts)
+    gpu.build_tree(8, 64)
+    gpu.compute_multipoles()
+    acc = gpu.walk_forces(bhg.Context.params(0.5, 0.0, 1.0, True, bhg.PRECISION_FP64), 0)
+    assert np.all(np.isfinite(acc))
+    out, racc, _ = oracle.step(parts, theta=0.5, eps2=0.0, max_leaf=8, group_size=64, target_size=0, want_acc=True)
+    assert rel_error(acc, racc) <= 1e-12
+
+
+def test_step_integrates_like_oracle(gpu, oracle):
+    parts = bhg.plummer(20000, 3)[0]
+    kw = dict(theta=0.5, eps2=1e-4, max_leaf=16, group_size=256, target_size=16)
+    ref, racc, _ = oracle.step(parts, kick_dt=1 / 256, drift_dt=1 / 128, want_acc=True, **kw)
+    gpu.upload(parts)
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, bhg.PRECISION_FP64)
+    gpu.step(fp, 16, 256, 16, 1 / 256, 1 / 128)
+    out = gpu.download()
+    assert np.array_equal(out["id"], ref["id"])
+    # positions/velocities move by dt * (a few e-16 relative force differences)
+    assert np.max(np.abs(out["vel"] - ref["vel"])) < 1e-12
+    assert np.max(np.abs(out["pos"] - ref["pos"])) < 1e-12
+
+
+def test_schedule_matches_oracle(gpu, oracle):
+    parts = bhg.plummer(8192, 4)[0]
+    dt, steps = 1 / 128, 3
+    kw = dict(theta=0.5, eps2=1e-4, max_leaf=16, group_size=256, target_size=16)
+    ref = parts
+    sched = [(dt / 2, dt)] + [(dt, dt)] * (steps - 1) + [(dt / 2, 0.0)]
+    for k, d in sched:
+        ref, _, _ = oracle.step(ref, kick_dt=k, drift_dt=d, **kw)
+    gpu.upload(parts)
+    gpu.run_schedule(bhg.Context.params(0.5, 1e-4, 1.0, True, bhg.PRECISION_FP64), 16, 256, 16, dt, steps)
+    out = gpu.download()
+    assert np.array_equal(out["id"], ref["id"])
+    assert np.max(np.abs(out["pos"] - ref["pos"])) < 1e-10
+
+
+def test_systems_match_one_at_a_time(gpu, oracle):
+    systems = [bhg.plummer(n, 100 + i, id0=0)[0] for i, n in enumerate((1500, 5000, 1024, 9000))]
+    gpu.upload_systems(systems)
+    th = np.array([0.5, 0.4, 0.7, 0.5])
+    e2 = np.array([1e-4, 1e-4, 2.5e-5, 1e-4])
+    gpu.set_system_params(theta=th, eps2=e2, kick_dt=np.full(4, 0.01), drift_dt=np.full(4, 0.02))
+    gpu.step_systems(bhg.Context.params(0.5, 1e-4, 1.0, True, bhg.PRECISION_FP64), 16, 256, 16)
+    out = gpu.download()
+    at = 0
+    for i, s in enumerate(systems):
+        ref, _, _ = oracle.step(s, theta=th[i], eps2=e2[i], kick_dt=0.01, drift_dt=0.02, max_leaf=16,
+                                group_size=256, target_size=16)
+        got = out[at:at + len(s)]
+        at += len(s)
+        assert np.array_equal(got["id"], ref["id"])
+        assert np.max(np.abs(got["pos"] - ref["pos"])) < 1e-12
+
+
+def test_direct_sum_matches_cpu(gpu, oracle):
+    parts = bhg.plummer(5000, 8)[0]
+    gpu.upload(parts)
+    idx = np.arange(0, 5000, 7, dtype=np.uint32)
+    got = gpu.direct_sum(idx, 1e-4)
+    ref = oracle.direct(soa(parts), idx, 1e-4)
+    assert rel_error(got, ref) < 1e-13
+
+
+def test_energy_matches_cpu(gpu, oracle):
+    parts = bhg.plummer(3000, 9)[0]
+    gpu.upload(parts)
+    k, p = gpu.energy()
+    assert abs(k - oracle.kinetic(parts)) <= 1e-12 * abs(k)
+    assert abs(p - oracle.potential(parts)) <= 1e-12 * abs(p)
+
+
+def test_nonfinite_input_is_rejected(gpu):
+    parts = cube(1000, 2)
+    parts["pos"][10, 1] = np.nan
+    gpu.upload(parts)
+    with pytest.raises(bhg.BhgError) as e:
+        gpu.build_tree(8, 64)
+    assert e.value.code == bhg.ENONFINITE
+    # the context stays usable
+    gpu.upload(cube(1000, 3))
+    gpu.build_tree(8, 64)
+
+
+def test_node_overflow_regrows(gpu, oracle):
+    # max_leaf 1 on tight clusters of 8: chains of single-child cells down to
+    # depth ~21 give far more nodes than the first estimate
+    parts = cube(4000, 12, spread=10.0)
+    parts["pos"] = np.repeat(parts["pos"][::8], 8, axis=0) + np.random.default_rng(3).uniform(-1e-7, 1e-7, (4000, 3))
+    gpu.upload(parts)
+    fp = bhg.Context.params(0.5, 1e-8, 1.0, True, bhg.PRECISION_FP64)
+    gpu.step(fp, 1, 64, 0, 0.0, 0.0)
+    out = gpu.download()
+    ref, _, _ = oracle.step(parts, theta=0.5, eps2=1e-8, max_leaf=1, group_size=64, target_size=0)
+    assert np.array_equal(out["id"], ref["id"])
