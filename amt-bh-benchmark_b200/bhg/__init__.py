@@ -53,12 +53,16 @@ class ForceParams(C.Structure):
 
 
 class Stats(C.Structure):
-    _fields_ = [("build_ms", C.c_double), ("multipole_ms", C.c_double), ("walk_ms", C.c_double),
-                ("sort_ms", C.c_double), ("pp", C.c_uint64), ("pc", C.c_uint64), ("nodes", C.c_uint32),
-                ("targets", C.c_uint32), ("depth", C.c_uint32), ("sort_passes", C.c_uint32)]
+    _fields_ = [("pre_ms", C.c_double), ("sort_ms", C.c_double), ("tree_ms", C.c_double),
+                ("multipole_ms", C.c_double), ("targets_ms", C.c_double), ("walk_ms", C.c_double),
+                ("last_walk_ms", C.c_double), ("pp", C.c_uint64), ("pc", C.c_uint64), ("evals", C.c_uint32),
+                ("nodes", C.c_uint32), ("targets", C.c_uint32), ("depth", C.c_uint32),
+                ("sort_passes", C.c_uint32), ("kernels_per_eval", C.c_uint32)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["build_ms"] = d["pre_ms"] + d["sort_ms"] + d["tree_ms"]
+        return d
 
 
 _lib = None
@@ -92,7 +96,7 @@ def lib() -> C.CDLL:
         "bhg_step_systems": ([vp, C.POINTER(ForceParams), C.c_uint, u32, u32], i32),
         "bhg_run_schedule": ([vp, C.POINTER(ForceParams), C.c_uint, u32, u32, f64, i32], i32),
         "bhg_set_system_params": ([vp, vp, vp, vp, vp], i32),
-        "bhg_get_stats": ([vp, C.POINTER(Stats)], i32),
+        "bhg_get_stats": ([vp, C.POINTER(Stats), i32], i32),
         "bhg_device_status": ([vp, C.POINTER(u32)], i32),
         "bhg_debug_export": ([vp, i32, vp, sz, C.POINTER(sz)], i32),
         "bhg_direct_sum": ([vp, i32, vp, sz, f64, f64, vp], i32),
@@ -241,9 +245,10 @@ class Context:
         arrs = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (theta, eps2, kick_dt, drift_dt)]
         self._ck(self.L.bhg_set_system_params(self.h, *[None if a is None else _p(a) for a in arrs]))
 
-    def stats(self) -> dict:
+    def stats(self, reset=True) -> dict:
+        """Phase times and interaction counts summed since the last reset."""
         s = Stats()
-        self._ck(self.L.bhg_get_stats(self.h, C.byref(s)))
+        self._ck(self.L.bhg_get_stats(self.h, C.byref(s), int(reset)))
         return s.as_dict()
 
     def device_status(self) -> int:

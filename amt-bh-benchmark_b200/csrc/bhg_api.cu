@@ -15,13 +15,10 @@ using namespace bhg;
 
 namespace {
 
-constexpr uint32_t kStackCap = 8192;  // per-warp walk stack (one pop per step beyond it)
-constexpr uint32_t kFatal = kStNonFinite | kStNodeOverflow | kStSpinLimit | kStTooLarge;
 
-enum Ev { kEvStart, kEvSortStart, kEvSortEnd, kEvBuildEnd, kEvMomEnd, kEvWalkStart, kEvWalkEnd, kEvCount };
-
-// Event record that also works inside stream capture (an event-record node).
-inline void rec(cudaEvent_t e, cudaStream_t s) { cudaEventRecordWithFlags(e, s, cudaEventRecordExternal); }
+// Phases of one evaluation, each timed with CUDA events and, in bhg_step,
+// replayed from its own captured graph.
+enum Phase { kPre, kSort, kTree, kMoments, kTargets, kWalk, kPhases };
 
 }  // namespace
 
@@ -55,7 +52,8 @@ struct bhg_context {
   SysDev* sys = nullptr;
   SysParam* prm = nullptr;
   Nodes nd{};
-  uint32_t *level_lb = nullptr, *mark = nullptr, *targets = nullptr, *scan_lb = nullptr, *stack = nullptr;
+  uint32_t *level_lb = nullptr, *mark = nullptr, *targets = nullptr, *scan_lb = nullptr;
+  uint32_t *groups = nullptr, *group_first = nullptr;
   double* accel = nullptr;
   DevState* st = nullptr;
   DevState* st_host = nullptr;  // pinned
@@ -67,13 +65,21 @@ struct bhg_context {
   int quad = 1, precision = 0;
   bool mask = false;
 
-  // timing
-  cudaEvent_t ev[kEvCount] = {};
-  bool timed_build = false, timed_walk = false;
+  // timing: CUDA events around every phase, summed on request
+  struct Pending {
+    int phase;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> ev_free, ev_all;
+  std::vector<Pending> pending;
+  cudaEvent_t open_ev = nullptr;  // boundary event after the last phase
+  double tot_ms[kPhases] = {};
+  double last_walk_ms = 0.0;
+  uint32_t walks_timed = 0;
 
-  // captured whole-step graph
-  cudaGraphExec_t graph = nullptr;
-  std::string graph_key;
+  // captured graphs, one per phase
+  cudaGraphExec_t graph[kPhases] = {};
+  std::string graph_key[kPhases];
 };
 
 namespace {
@@ -125,9 +131,11 @@ int grow(bhg_context* c, T** p, size_t count) {
 }
 
 void drop_graph(bhg_context* c) {
-  if (c->graph) cudaGraphExecDestroy(c->graph);
-  c->graph = nullptr;
-  c->graph_key.clear();
+  for (int p = 0; p < kPhases; ++p) {
+    if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
+    c->graph[p] = nullptr;
+    c->graph_key[p].clear();
+  }
 }
 
 // Node slots for n particles: about 0.25 per particle at max_leaf 16 on
@@ -145,7 +153,8 @@ int ensure_nodes(bhg_context* c, size_t need) {
   if ((r = grow(c, &c->nd.begin, cap)) || (r = grow(c, &c->nd.count, cap)) || (r = grow(c, &c->nd.first, cap)) ||
       (r = grow(c, &c->nd.info, cap)) || (r = grow(c, &c->nd.box, cap)) || (r = grow(c, &c->nd.mom, cap)) ||
       (r = grow(c, &c->nd.iab, cap * 6)) || (r = grow(c, &c->nd.w, cap)) || (r = grow(c, &c->nd.q45, cap)) ||
-      (r = grow(c, &c->nd.q64, cap * 6)) || (r = grow(c, &c->targets, cap)) ||
+      (r = grow(c, &c->nd.q64, cap * 6)) || (r = grow(c, &c->targets, cap)) || (r = grow(c, &c->groups, cap)) ||
+      (r = grow(c, &c->group_first, cap)) ||
       (r = grow(c, &c->level_lb, cap / 32 + kLevels + 8)))
     return r;
   c->nd.cap = (uint32_t)cap;
@@ -162,7 +171,7 @@ int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles) {
     c->accel = nullptr;
     if ((r = grow(c, &c->part, n)) || (r = grow(c, &c->staged, n)) || (r = grow(c, &c->pm, n)) ||
         (r = grow(c, &c->keys[0], n)) || (r = grow(c, &c->keys[1], n)) || (r = grow(c, &c->vals[0], n)) ||
-        (r = grow(c, &c->vals[1], n)) || (r = grow(c, &c->mark, n)) || (r = grow(c, &c->scan_lb, n / 4096 + 8)))
+        (r = grow(c, &c->vals[1], n)) || (r = grow(c, &c->mark, n)) || (r = grow(c, &c->scan_lb, 2 * (n / 4096) + 32)))
       return r;
     CK(cudaMemsetAsync(c->mark, 0xff, n * sizeof(uint32_t), c->stream));
     c->cap_n = n;
@@ -190,12 +199,10 @@ int walk_grid(bhg_context* c) {
 }
 
 int ensure_stack(bhg_context* c, int grid) {
+  // the walk keeps its stacks in shared memory; this only makes sure the
+  // kernel's occupancy (and shared-memory limit) is set up before capture
   size_t warps = (size_t)grid * (walk_threads() / 32);
-  if (warps <= c->cap_stack_warps) return BHG_OK;
-  drop_graph(c);
-  int r = grow(c, &c->stack, warps * kStackCap);
-  if (r) return r;
-  c->cap_stack_warps = warps;
+  c->cap_stack_warps = std::max(c->cap_stack_warps, warps);
   return BHG_OK;
 }
 
@@ -240,39 +247,45 @@ int set_problem(bhg_context* c, const uint64_t* counts, size_t nsys) {
 
 // ---- enqueue the phases (no host synchronisation) ---------------------------
 
-void enq_build(bhg_context* c, bool timed) {
+void enq_pre(bhg_context* c) {
   cudaStream_t s = c->stream;
   const int nt = (int)c->tiles_host.size();
-  if (timed) rec(c->ev[kEvStart], s);
   cudaMemsetAsync(reinterpret_cast<char*>(c->st) + kBuildResetOffset, 0, sizeof(DevState) - kBuildResetOffset, s);
   cudaMemsetAsync(c->hist, 0, (size_t)c->nsys * kSortPasses * 256 * sizeof(uint32_t), s);
   cudaMemsetAsync(c->sort_lb, 0, (size_t)nt * kSortPasses * 256 * sizeof(uint32_t), s);
   cudaMemsetAsync(c->level_lb, 0, (c->cap_nodes / 32 + kLevels + 8) * sizeof(uint32_t), s);
   launch_bounds_domain(c->part, c->tiles, nt, c->sys, c->nsys, c->partial, c->st, s);
   launch_keys(c->part, c->tiles, nt, c->sys, c->nsys, c->keys[0], c->hist, c->offs, s);
-  if (timed) rec(c->ev[kEvSortStart], s);
+}
+
+void enq_sort(bhg_context* c) {
+  const int nt = (int)c->tiles_host.size();
   for (int p = 0; p < kSortPasses; ++p)
     launch_sort_pass(c->keys[p & 1], c->vals[p & 1], c->keys[(p + 1) & 1], c->vals[(p + 1) & 1], p, c->tiles, nt,
-                     c->offs, c->sort_lb + (size_t)p * nt * 256, c->st, s);
-  if (timed) rec(c->ev[kEvSortEnd], s);
+                     c->offs, c->sort_lb + (size_t)p * nt * 256, c->st, c->stream);
+}
+
+void enq_tree(bhg_context* c) {
   // kSortPasses is even: sorted keys and the permutation are back in [0]
-  launch_gather(c->part, c->vals[0], (uint32_t)c->n, c->staged, c->pm, c->sms, s);
-  launch_topology(c->sys, c->nsys, c->nd, c->keys[0], c->max_leaf, c->level_lb, c->st, c->sms, s);
-  if (timed) rec(c->ev[kEvBuildEnd], s);
+  launch_gather(c->part, c->vals[0], (uint32_t)c->n, c->staged, c->pm, c->sms, c->stream);
+  launch_topology(c->sys, c->nsys, c->nd, c->keys[0], c->max_leaf, c->level_lb, c->st, c->sms, c->stream);
 }
 
-void enq_moments(bhg_context* c, bool timed) {
-  launch_moments(c->nd, c->pm, c->st, c->sms, c->stream);
-  if (timed) rec(c->ev[kEvMomEnd], c->stream);
-}
+void enq_moments(bhg_context* c) { launch_moments(c->nd, c->pm, c->st, c->sms, c->stream); }
 
-void enq_walk(bhg_context* c, uint32_t target_size, bool timed, bool want_accel) {
+void enq_targets(bhg_context* c, uint32_t target_size) {
   cudaStream_t s = c->stream;
   cudaMemsetAsync(reinterpret_cast<char*>(c->st) + kWalkResetOffset, 0, sizeof(DevState) - kWalkResetOffset, s);
-  cudaMemsetAsync(c->scan_lb, 0, (c->n / 4096 + 8) * sizeof(uint32_t), s);
-  const uint32_t gs = c->group_size == 0 ? 0u : c->group_size;
-  const uint32_t lim = std::min(target_size, gs);
-  launch_targets(c->nd, lim, (uint32_t)c->n, c->mark, c->targets, c->scan_lb, c->st, c->sms, s);
+  cudaMemsetAsync(c->scan_lb, 0, (2 * (c->n / 4096) + 32) * sizeof(uint32_t), s);
+  const uint32_t lim = std::min(target_size, c->group_size);
+  // walk groups share the upper walk of their targets; with targets above
+  // kGroupMax particles every target is its own group
+  const uint32_t glim = std::max<uint32_t>(lim, kGroupMax);
+  launch_targets(c->nd, lim, glim, (uint32_t)c->n, c->mark, c->targets, c->groups, c->group_first, c->scan_lb, c->st,
+                 c->sms, s);
+}
+
+void enq_walk(bhg_context* c, bool want_accel) {
   WalkArgs a;
   a.w = c->nd.w;
   a.q45 = c->nd.q45;
@@ -282,24 +295,112 @@ void enq_walk(bhg_context* c, uint32_t target_size, bool timed, bool want_accel)
   a.ncount = c->nd.count;
   a.pm = c->pm;
   a.targets = c->targets;
+  a.groups = c->groups;
+  a.group_first = c->group_first;
   a.sys = c->sys;
   a.prm = c->prm;
   a.nsys = c->nsys;
   a.staged = c->staged;
   a.out = c->part;
   a.accel = want_accel ? c->accel : nullptr;
-  a.stack = c->stack;
-  a.stack_cap = kStackCap;
   a.st = c->st;
-  if (timed) rec(c->ev[kEvWalkStart], s);
-  launch_walk(a, c->precision, c->quad != 0, c->mask, walk_grid(c), s);
-  if (timed) rec(c->ev[kEvWalkEnd], s);
-  launch_eval_done(c->st, s);
+  launch_walk(a, c->precision, c->quad != 0, c->mask, walk_grid(c), c->stream);
+  launch_eval_done(c->st, c->stream);
+}
+
+// ---- phase timing -------------------------------------------------------------
+
+cudaEvent_t take_event(bhg_context* c) {
+  if (c->ev_free.empty()) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    c->ev_all.push_back(e);
+    return e;
+  }
+  cudaEvent_t e = c->ev_free.back();
+  c->ev_free.pop_back();
+  return e;
+}
+
+// Folds every recorded phase time into the sums (blocks) and recycles events.
+void fold_times(bhg_context* c) {
+  cudaStreamSynchronize(c->stream);
+  for (const auto& p : c->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      c->tot_ms[p.phase] += ms;
+      if (p.phase == kWalk) {
+        c->last_walk_ms = ms;
+        ++c->walks_timed;
+      }
+    } else {
+      cudaGetLastError();
+    }
+  }
+  c->pending.clear();
+  c->ev_free = c->ev_all;
+  c->open_ev = nullptr;
+}
+
+// Runs `enq` as phase `phase`: from a captured graph when `graphed`, with a
+// CUDA event before and after it on the stream.
+template <typename F>
+int run_phase(bhg_context* c, int phase, bool graphed, const std::string& key, F enq) {
+  if (c->pending.size() > 16384) fold_times(c);
+  if (!c->open_ev) {
+    c->open_ev = take_event(c);
+    CK(cudaEventRecord(c->open_ev, c->stream));
+  }
+  cudaEvent_t a = c->open_ev;
+  if (graphed) {
+    if (!c->graph[phase] || c->graph_key[phase] != key) {
+      if (c->graph[phase]) cudaGraphExecDestroy(c->graph[phase]);
+      c->graph[phase] = nullptr;
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      enq();
+      CK(cudaStreamEndCapture(c->stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&c->graph[phase], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        c->graph[phase] = nullptr;
+        return fail(c, BHG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      }
+      c->graph_key[phase] = key;
+    }
+    CK(cudaGraphLaunch(c->graph[phase], c->stream));
+  } else {
+    enq();
+    CK(cudaGetLastError());
+  }
+  cudaEvent_t b = take_event(c);
+  CK(cudaEventRecord(b, c->stream));
+  c->pending.push_back({phase, a, b});
+  c->open_ev = b;
+  return BHG_OK;
+}
+
+std::string graph_key(const bhg_context* c, uint32_t target_size) {
+  char key[192];
+  snprintf(key, sizeof key, "%zu/%d/%zu/%zu/%u/%u/%u/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->cap_stack_warps,
+           c->max_leaf, c->group_size, target_size, c->precision, c->quad, (int)c->mask);
+  return key;
+}
+
+// The three build phases (bhg_build_tree).
+int run_build(bhg_context* c, bool graphed, const std::string& key) {
+  int r;
+  if ((r = run_phase(c, kPre, graphed, key, [&] { enq_pre(c); })) ||
+      (r = run_phase(c, kSort, graphed, key, [&] { enq_sort(c); })) ||
+      (r = run_phase(c, kTree, graphed, key, [&] { enq_tree(c); })))
+    return r;
+  return BHG_OK;
 }
 
 int push_params(bhg_context* c) {
   CK(cudaMemcpyAsync(c->prm, c->prm_host.data(), c->prm_host.size() * sizeof(SysParam), cudaMemcpyHostToDevice,
                      c->stream));
+  c->open_ev = nullptr;  // the copy is not part of any phase
   return BHG_OK;
 }
 
@@ -315,6 +416,7 @@ std::string status_text(uint32_t s) {
   if (s & kStNodeOverflow) t += " octree larger than its node slots;";
   if (s & kStSpinLimit) t += " a bounded wait in a sort/scan kernel gave up;";
   if (s & kStTooLarge) t += " a count exceeded 30 bits;";
+  if (s & kStWalkLimit) t += " a walk visited more nodes than the tree holds;";
   return t;
 }
 
@@ -379,7 +481,6 @@ int bhg_create(bhg_context** out, const bhg_config* cfg) {
     return BHG_ECUDA;
   }
   c->own_stream = true;
-  for (auto& ev : c->ev) cudaEventCreate(&ev);
   set_build_attributes();
   if (dev_alloc(c, reinterpret_cast<void**>(&c->st), sizeof(DevState)) ||
       cudaMallocHost(&c->st_host, sizeof(DevState)) != cudaSuccess) {
@@ -399,7 +500,7 @@ int bhg_destroy(bhg_context* c) {
   for (auto& a : c->allocs) cudaFree(a.first);
   c->allocs.clear();
   if (c->st_host) cudaFreeHost(c->st_host);
-  for (auto& ev : c->ev)
+  for (auto& ev : c->ev_all)
     if (ev) cudaEventDestroy(ev);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -411,7 +512,7 @@ const char* bhg_last_error(const bhg_context* c) { return c ? c->err.c_str() : "
 int bhg_set_stream(bhg_context* c, void* s) {
   if (!c) return BHG_EINVAL;
   cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
+  fold_times(c);
   drop_graph(c);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   if (s) {
@@ -475,12 +576,11 @@ int bhg_build_tree(bhg_context* c, unsigned max_leaf, uint32_t group_size) {
   c->group_size = group_size;
   int r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf));
   if (r) return r;
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    enq_build(c, true);
-    c->timed_build = true;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    if ((r = run_build(c, false, ""))) return r;
     if ((r = read_state(c))) return r;
     if (c->st_host->status & kStNodeOverflow) {
-      size_t need = (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64;
+      size_t need = std::max<size_t>(2 * c->cap_nodes, (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64);
       if ((r = clear_status(c)) || (r = ensure_nodes(c, need))) return r;
       continue;
     }
@@ -499,8 +599,8 @@ int bhg_compute_multipoles(bhg_context* c) {
   if (!c) return BHG_EINVAL;
   if (!c->built) return fail(c, BHG_ESTATE, "build the tree first");
   cudaSetDevice(c->device);
-  rec(c->ev[kEvBuildEnd], c->stream);
-  enq_moments(c, true);
+  int r = run_phase(c, kMoments, false, "", [&] { enq_moments(c); });
+  if (r) return r;
   c->moments = true;
   return BHG_OK;
 }
@@ -514,8 +614,9 @@ int bhg_walk_forces(bhg_context* c, const bhg_force_params* fp, uint32_t target_
   if (r) return r;
   if (!c->accel && (r = grow(c, &c->accel, c->cap_n * 3))) return r;
   if ((r = ensure_stack(c, walk_grid(c))) || (r = push_params(c))) return r;
-  enq_walk(c, target_size, true, true);
-  c->timed_walk = true;
+  if ((r = run_phase(c, kTargets, false, "", [&] { enq_targets(c, target_size); })) ||
+      (r = run_phase(c, kWalk, false, "", [&] { enq_walk(c, true); })))
+    return r;
   c->walked = true;
   c->moments = false;  // the state moved: the next walk needs a new build
   c->built = false;
@@ -564,28 +665,15 @@ int bhg_set_system_params(bhg_context* c, const double* theta, const double* eps
 
 namespace {
 
-// One whole evaluation (build + multipoles + walk), replayed from a graph.
-int enq_step(bhg_context* c, uint32_t target_size, bool timed) {
-  char key[160];
-  snprintf(key, sizeof key, "%zu/%d/%zu/%u/%u/%u/%d/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->max_leaf,
-           c->group_size, target_size, c->precision, c->quad, (int)c->mask, (int)timed);
-  if (!c->graph || c->graph_key != key) {
-    drop_graph(c);
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    enq_build(c, timed);
-    enq_moments(c, timed);
-    enq_walk(c, target_size, timed, false);
-    CK(cudaStreamEndCapture(c->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-      c->graph = nullptr;
-      return fail(c, BHG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    }
-    c->graph_key = key;
-  }
-  CK(cudaGraphLaunch(c->graph, c->stream));
+// One whole evaluation (build + multipoles + walk), each phase replayed from
+// its captured graph.
+int enq_step(bhg_context* c, uint32_t target_size) {
+  const std::string key = graph_key(c, target_size);
+  int r;
+  if ((r = run_build(c, true, key)) || (r = run_phase(c, kMoments, true, key, [&] { enq_moments(c); })) ||
+      (r = run_phase(c, kTargets, true, key, [&] { enq_targets(c, target_size); })) ||
+      (r = run_phase(c, kWalk, true, key, [&] { enq_walk(c, false); })))
+    return r;
   return BHG_OK;
 }
 
@@ -609,7 +697,7 @@ int prepare_step(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, 
 // evaluation that failed (its walk was skipped, so the state is intact).
 int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<double, double>>& kd, bool keep) {
   size_t next = 0;
-  for (int attempt = 0; attempt < 6; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     int r;
     if ((r = read_state(c))) return r;
     const uint32_t base = c->st_host->evals_ok;
@@ -620,19 +708,18 @@ int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<
           p.drift_dt = kd[i].second;
         }
       }
-      if ((r = push_params(c)) || (r = enq_step(c, target_size, true))) return r;
+      if ((r = push_params(c)) || (r = enq_step(c, target_size))) return r;
     }
     if ((r = read_state(c))) return r;
     const uint32_t done = c->st_host->evals_ok - base;
     if (c->st_host->status == 0) {
-      c->timed_build = c->timed_walk = true;
       c->walked = true;
       c->built = c->moments = false;
       return BHG_OK;
     }
     if (c->st_host->status & kStNodeOverflow) {
       next += done;
-      size_t need = (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64;
+      size_t need = std::max<size_t>(2 * c->cap_nodes, (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64);
       if ((r = clear_status(c)) || (r = ensure_nodes(c, need)) || (r = ensure_stack(c, walk_grid(c)))) return r;
       continue;
     }
@@ -676,32 +763,38 @@ int bhg_run_schedule(bhg_context* c, const bhg_force_params* fp, unsigned max_le
   return run_evals(c, target_size, kd, false);
 }
 
-int bhg_get_stats(bhg_context* c, bhg_stats* out) {
+int bhg_get_stats(bhg_context* c, bhg_stats* out, int reset) {
   if (!c || !out) return BHG_EINVAL;
   cudaSetDevice(c->device);
+  fold_times(c);
   int r = read_state(c);
   if (r) return r;
   std::memset(out, 0, sizeof *out);
-  float ms = 0.f;
-  auto el = [&](int a, int b) -> double {
-    if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) {
-      cudaGetLastError();
-      return -1.0;
-    }
-    return ms;
-  };
-  if (c->timed_build) {
-    out->build_ms = el(kEvStart, kEvBuildEnd);
-    out->sort_ms = el(kEvSortStart, kEvSortEnd);
-    out->multipole_ms = el(kEvBuildEnd, kEvMomEnd);
-  }
-  if (c->timed_walk) out->walk_ms = el(kEvWalkStart, kEvWalkEnd);
-  out->pp = c->st_host->pp;
-  out->pc = c->st_host->pc;
+  out->pre_ms = c->tot_ms[kPre];
+  out->sort_ms = c->tot_ms[kSort];
+  out->tree_ms = c->tot_ms[kTree];
+  out->multipole_ms = c->tot_ms[kMoments];
+  out->targets_ms = c->tot_ms[kTargets];
+  out->walk_ms = c->tot_ms[kWalk];
+  out->last_walk_ms = c->last_walk_ms;
+  out->evals = c->walks_timed;
+  out->pp = c->st_host->pp_total;
+  out->pc = c->st_host->pc_total;
   out->nodes = c->st_host->n_nodes;
   out->targets = c->st_host->n_targets;
   out->depth = c->st_host->max_depth;
   out->sort_passes = kSortPasses;
+  // bounds + domain + keys + digit offsets; the sort passes; gather + roots +
+  // one per level; one multipole kernel per level; mark + compact of the
+  // targets and of the groups + first target per group; walk + its
+  // completion count
+  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (kMortonDepth + 1) + 5 + 2;
+  if (reset) {
+    for (double& t : c->tot_ms) t = 0.0;
+    c->walks_timed = 0;
+    CK(cudaMemsetAsync(&c->st->pp_total, 0, 2 * sizeof(unsigned long long), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   return BHG_OK;
 }
 

@@ -382,6 +382,10 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(int depth, Nodes nd, co
   __shared__ uint32_t s_base;
   const uint32_t pb = st->level_begin[depth - 1], pc = st->level_count[depth - 1];
   const uint32_t cb = pb + pc;  // level_begin[depth]
+  if (cb > nd.cap) {  // an earlier level overflowed the slots: nothing to read here
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&st->status, kStNodeOverflow);
+    return;
+  }
   const uint32_t ntiles = (pc + kLevelParents - 1) / kLevelParents;
   uint32_t* lookback = lookback_all + pb / kLevelParents + depth;
   const int tid = threadIdx.x, lane = tid & 31, oct = tid & 7;
@@ -468,11 +472,14 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(int depth, Nodes nd, co
 }
 
 // ---------------------------------------------------------------------------
-// walk targets: the topmost nodes that are leaves or hold at most `lim`
-// particles (lim = min(target_size, group_size); see bhg_kernels.h), marked
-// at their first particle and compacted in Morton order.
+// Cuts of the tree: the topmost nodes that are leaves or hold at most `lim`
+// particles, marked at their first particle and compacted in Morton order.
+// Used twice per walk: for the walk targets (lim = min(target_size,
+// group_size)) and for the walk groups (lim = kGroupMax), the nodes whose
+// targets share the upper part of their walk.
 
-__global__ void k_mark_targets(Nodes nd, uint32_t lim, const DevState* __restrict__ st, uint32_t* __restrict__ mark) {
+__global__ void k_mark_cut(Nodes nd, uint32_t lim, const DevState* __restrict__ st, uint32_t* __restrict__ mark) {
+  if (st->status & kStNodeOverflow) return;  // children may lie beyond the slots
   const uint32_t nn = min(st->n_nodes, nd.cap), nroots = st->level_count[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
     const uint32_t info = nd.info[i], cnt = nd.count[i];
@@ -482,6 +489,7 @@ __global__ void k_mark_targets(Nodes nd, uint32_t lim, const DevState* __restric
       const uint32_t f = nd.first[i], k = info_nchild(info);
       for (uint32_t j = 0; j < k; ++j) {
         const uint32_t ch = f + j;
+        if (ch >= nd.cap) break;
         if (info_leaf(nd.info[ch]) || nd.count[ch] <= lim) mark[nd.begin[ch]] = ch;
       }
     }
@@ -491,14 +499,17 @@ __global__ void k_mark_targets(Nodes nd, uint32_t lim, const DevState* __restric
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 
-__global__ void __launch_bounds__(kScanThreads) k_compact_targets(uint32_t* __restrict__ mark, uint32_t n,
-                                                                  uint32_t* __restrict__ targets,
-                                                                  uint32_t* __restrict__ lookback, DevState* st) {
+// Compacts the marked entries of mark[0..n) into out (Morton order), resets
+// the marks, and writes the count.  Tiles chain through a decoupled look-back.
+__global__ void __launch_bounds__(kScanThreads) k_compact(uint32_t* __restrict__ mark, uint32_t n,
+                                                          uint32_t* __restrict__ out, uint32_t* __restrict__ lookback,
+                                                          uint32_t* tile_counter, uint32_t* count_out,
+                                                          DevState* st) {
   __shared__ uint32_t s_tile, s_base;
   __shared__ uint32_t s_scan[kScanThreads / 32 + 2];
   const uint32_t ntiles = (n + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
   for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&st->scan_tiles, 1u);
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
     if (tile >= ntiles) break;
@@ -519,16 +530,34 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_targets(uint32_t* __re
         st_volatile(&lookback[tile], kFlagPre | (excl + total));
       }
       s_base = excl;
-      if (tile == ntiles - 1) st->n_targets = excl + total;
+      if (tile == ntiles - 1) *count_out = excl + total;
     }
     __syncthreads();
     uint32_t o = s_base + ex;
 #pragma unroll
     for (int j = 0; j < kScanItems; ++j) {
-      if (v[j] != 0xffffffffu) targets[o++] = v[j];
-      if (base + j < n) mark[base + j] = 0xffffffffu;  // ready for the next step
+      if (v[j] != 0xffffffffu) out[o++] = v[j];
+      if (base + j < n) mark[base + j] = 0xffffffffu;  // ready for the next use
     }
     __syncthreads();
+  }
+}
+
+// first_target[g]: index of the first target inside group g (targets and
+// groups are both in Morton order and every target lies inside one group).
+__global__ void k_group_first(const uint32_t* __restrict__ groups, const uint32_t* __restrict__ targets,
+                              const uint32_t* __restrict__ nbegin, const DevState* __restrict__ st,
+                              uint32_t* __restrict__ first_target) {
+  const uint32_t ng = st->n_groups, nt = st->n_targets;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    const uint32_t gb = nbegin[groups[g]];
+    uint32_t lo = 0, hi = nt;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (nbegin[targets[mid]] < gb) lo = mid + 1;
+      else hi = mid;
+    }
+    first_target[g] = lo;
   }
 }
 
@@ -563,6 +592,7 @@ __device__ __forceinline__ void raw_add(Raw& r, double m, const double d[3], con
 }
 
 __global__ void k_moments(int depth, Nodes nd, const double4* __restrict__ pm, const DevState* __restrict__ st) {
+  if (st->status & kStNodeOverflow) return;  // children may lie beyond the slots
   const uint32_t lb = st->level_begin[depth];
   const uint32_t lc = depth < (int)st->max_depth ? st->level_count[depth] : 0u;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < lc; k += gridDim.x * blockDim.x) {
@@ -678,10 +708,16 @@ void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_
     k_level<<<sms * 4, kLevelThreads, 0, s>>>(d, nd, keys, max_leaf, lookback, st);
 }
 
-void launch_targets(const Nodes& nd, uint32_t lim, uint32_t n, uint32_t* mark, uint32_t* targets,
-                    uint32_t* lookback, DevState* st, int sms, cudaStream_t s) {
-  k_mark_targets<<<sms * 4, 256, 0, s>>>(nd, lim, st, mark);
-  k_compact_targets<<<sms * 2, kScanThreads, 0, s>>>(mark, n, targets, lookback, st);
+void launch_targets(const Nodes& nd, uint32_t lim, uint32_t group_lim, uint32_t n, uint32_t* mark, uint32_t* targets,
+                    uint32_t* groups, uint32_t* first_target, uint32_t* lookback, DevState* st, int sms,
+                    cudaStream_t s) {
+  const uint32_t ntiles = (n + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+  k_mark_cut<<<sms * 4, 256, 0, s>>>(nd, lim, st, mark);
+  k_compact<<<sms * 2, kScanThreads, 0, s>>>(mark, n, targets, lookback, &st->scan_tiles, &st->n_targets, st);
+  k_mark_cut<<<sms * 4, 256, 0, s>>>(nd, group_lim, st, mark);
+  k_compact<<<sms * 2, kScanThreads, 0, s>>>(mark, n, groups, lookback + ntiles + 8, &st->group_tiles,
+                                             &st->n_groups, st);
+  k_group_first<<<sms * 2, 256, 0, s>>>(groups, targets, nd.begin, st, first_target);
 }
 
 void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, cudaStream_t s) {

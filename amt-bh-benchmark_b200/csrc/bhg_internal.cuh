@@ -30,6 +30,7 @@ enum : uint32_t {
   kStNodeOverflow = 1u << 1,  // more nodes than node slots: grow and redo
   kStSpinLimit = 1u << 2,     // a bounded wait gave up
   kStTooLarge = 1u << 3,      // a count exceeded a 30-bit field
+  kStWalkLimit = 1u << 4,     // a walk visited more nodes than the tree holds
 };
 
 struct alignas(64) Particle {  // bh::Particle, particle.h:7-24
@@ -84,6 +85,7 @@ struct DevState {
   // sticky: cleared by the host only
   uint32_t status;    // error bits; while set, walks skip and the state stays put
   uint32_t evals_ok;  // evaluations that finished with status 0
+  unsigned long long pp_total, pc_total;  // interactions of those evaluations
   // per build (zeroed by every build)
   uint32_t n_nodes;  // total nodes (may exceed the slots on overflow)
   uint32_t max_depth;
@@ -93,8 +95,10 @@ struct DevState {
   uint32_t sort_tiles[16];            // tiles taken by each sort pass
   // per walk (zeroed by every walk)
   uint32_t n_targets;
-  uint32_t walk_next;        // next target of the walk
+  uint32_t n_groups;         // walk groups (nodes whose targets share a walk)
+  uint32_t walk_next;        // next group of the walk
   uint32_t scan_tiles;       // tiles taken by the target compaction
+  uint32_t group_tiles;      // tiles taken by the group compaction
   uint32_t pad0;
   unsigned long long pp, pc;  // interaction counts of the walk
 };
@@ -138,5 +142,6 @@ struct Nodes {
 // Kernel-launch helpers shared by the .cu files (defined in bhg_build.cu).
 constexpr int kTile = 4096;  // particles per radix-sort / bounds tile
 constexpr int kSortPasses = 8;
+constexpr int kGroupMax = 64;  // particles of a walk group (targets sharing one upper walk)
 
 }  // namespace bhg

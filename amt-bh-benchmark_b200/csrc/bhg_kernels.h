@@ -25,9 +25,12 @@ void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_
 // holds at most target_size particles (grouped_ttg.h:253); on every
 // root-to-leaf path that is the deeper of the two cuts, i.e. the first node
 // with count <= min(target_size, group_size).  group_size 0 (the per-node
-// pass) and target_size 0 both give the leaves.
-void launch_targets(const Nodes& nd, uint32_t lim, uint32_t n, uint32_t* mark, uint32_t* targets,
-                    uint32_t* lookback, DevState* st, int sms, cudaStream_t s);
+// pass) and target_size 0 both give the leaves.  The walk groups are the
+// same cut at group_lim (>= lim): the nodes whose targets share the upper
+// part of one walk; first_target[g] is the index of group g's first target.
+void launch_targets(const Nodes& nd, uint32_t lim, uint32_t group_lim, uint32_t n, uint32_t* mark, uint32_t* targets,
+                    uint32_t* groups, uint32_t* first_target, uint32_t* lookback, DevState* st, int sms,
+                    cudaStream_t s);
 void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, cudaStream_t s);
 
 struct WalkArgs {
@@ -39,14 +42,14 @@ struct WalkArgs {
   const uint32_t* ncount;
   const double4* pm;
   const uint32_t* targets;
+  const uint32_t* groups;
+  const uint32_t* group_first;  // first target of each group
   const SysDev* sys;
   const SysParam* prm;
   int nsys;
   const Particle* staged;  // Morton-ordered input of this step
   Particle* out;           // kicked/drifted particles (the state)
   double* accel;           // optional: G*a, 3 per particle
-  uint32_t* stack;         // per-warp traversal stacks
-  uint32_t stack_cap;
   DevState* st;
 };
 

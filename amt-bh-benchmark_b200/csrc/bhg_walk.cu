@@ -1,48 +1,65 @@
-// Force walk of the B200 Barnes-Hut path: one warp per target node.
+// Force walk of the B200 Barnes-Hut path.
 //
-// What a target receives is the reference's interaction list
-// (GroupWalker, grouped_ttg.h:204-289, which produces exactly the list of a
-// separate walk from the root per target, :42-51): the bounding box of the
-// target's particles (BBox, multipole.h:115-142) is tested against every
-// visited node with mac_accept_bbox (multipole.h:151-153), strict
-// theta^2 near^2 > edge^2 in FP64; leaves are tested too; accepted nodes are
-// cell interactions (quadrupole, accel_from_source multipole.h:171-200, or
-// monopoles in no-quad mode); everything else is opened - interior nodes
-// push their children, leaves contribute their particles directly, the
-// target's own leaf included (its self term is 0 with softening and masked
-// at r^2 = 0 without, accumulate_list grouped_ttg.h:117-163).
+// What a target receives is exactly the reference's interaction list
+// (GroupWalker, grouped_ttg.h:204-289): the bounding box of the target's
+// particles (BBox, multipole.h:115-142) is tested against the visited nodes
+// with mac_accept_bbox (multipole.h:151-153, strict theta^2 near^2 > edge^2,
+// in FP64); leaves are tested too; accepted nodes are cell interactions
+// (quadrupole, accel_from_source multipole.h:171-200, or monopoles in
+// no-quad mode); everything else is opened - interior nodes push their
+// children, leaves contribute their particles directly, the target's own
+// leaf included (its self term is 0 with softening and masked at r^2 = 0
+// without, accumulate_list grouped_ttg.h:117-163).
 //
-// The traversal is warp-cooperative: each step pops up to 32 nodes (one per
-// lane) from a per-warp stack, accepted cells and opened leaves' particles
-// are appended to two small shared-memory queues, and every time a queue
-// holds a full chunk the chunk is evaluated with one SOURCE PER LANE against
-// all of the target's particles held in registers (lanes = sources, loop =
-// targets), so all 32 lanes stay busy for any target size.  Up to 8 targets
-// per lane (FP32) or 4 (FP64); larger targets split the warp into 2-8 lane
-// groups that share each source chunk, and targets above 32 particles walk
-// once per 32.
+// One warp per walk GROUP (the topmost nodes with at most kGroupMax
+// particles, or leaves), sharing the upper walk among the group's targets as
+// GroupWalker::visit does: a first walk with the group's bounding box
+// resolves every node that is accepted for the whole box (then accepted for
+// every target inside it) or rejected for every point of it (mac_reject_all,
+// multipole.h:158-160: then opened by every target), evaluating those
+// interactions once against all of the group's particles; the rest is
+// deferred, and each target then walks only from the deferred nodes.  Each
+// target's list is the same as a separate walk from the root would build.
 //
-// Split precision: source and target positions become FP32 offsets from the
-// target's bounding-box centre (the subtraction in FP64), interactions are
-// FP32 FMA + rsqrtf, and every kFlushChunks chunks the per-lane FP32 partial
-// sums are reduced across the lane group and added to an FP64 accumulator
-// owned by one lane per target (compensated summation across list chunks).
-// The kick/drift of integrate_ttg.h:74-77 is applied in FP64 in the epilogue.
+// A walk step pops up to 32 nodes (one per lane) from a shared-memory stack;
+// accepted cells and opened leaves' particles go to two shared-memory
+// queues, and each full queue chunk is evaluated with one SOURCE PER LANE
+// against targets held in registers (up to 8 per lane; the warp splits into
+// 1-8 lane groups for up to 64 targets), so all lanes stay busy for any
+// target size.  The per-chunk bodies are specialised on the number of live
+// target slots so the independent interactions interleave.
+//
+// Split precision: sources and targets become FP32 offsets from the walk's
+// bounding-box centre (the subtraction in FP64), interactions are FP32 FMA
+// + rsqrtf, and every kFlushChunks chunks the FP32 partial sums are reduced
+// across the lane group into an FP64 sum owned by one lane per target
+// (compensated summation across list chunks).  The kick/drift of
+// integrate_ttg.h:74-77 is applied in FP64 in the epilogue.
 #include "bhg_kernels.h"
+
+#include <type_traits>
 
 namespace bhg {
 
 constexpr int kWalkWarps = 4;
 constexpr int kWalkThreads = kWalkWarps * 32;
-constexpr int kQueue = 64;
+constexpr int kQueue = 128;  // ring of queued sources: a chunk is 2 per lane
+constexpr int kStackCap = 1280;  // per-warp shared-memory stack
+constexpr int kDeferCap = 1024;  // per-warp deferred nodes of a group walk
 constexpr int kFlushChunks = 16;
 constexpr float kFarAway = 1.0e10f;  // padding source: contributes exactly 0
 constexpr uint32_t kFull = 0xffffffffu;
+static_assert(kStackCap >= kDeferCap + 7 * kLevels + 1 + 32, "a DFS walk from the deferred nodes must fit");
 
-struct WarpQueues {
+struct WarpSmem {
+  uint32_t stack[kStackCap];
+  uint32_t defer[kDeferCap];
   uint32_t cell[kQueue];
   uint32_t part[kQueue];
+  double acc[kGroupMax][3];   // FP64 sum per particle of the group
+  double tacc[kGroupMax][3];  // FP64 sums of one target's own walk
 };
+constexpr size_t kWalkSmem = sizeof(WarpSmem) * kWalkWarps;
 
 __device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v, int lane) {
 #pragma unroll
@@ -53,7 +70,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v, int lane) {
   return v;
 }
 
-// Squared distance from (x, y, z) to the nearest point of the box, exactly as
+// Squared distance from (x, y, z) to the nearest point of the box, as
 // BBox::near2 (multipole.h:132-136) rounds it.
 __device__ __forceinline__ double near2(const double lo[3], const double hi[3], double x, double y, double z) {
   double dx = fmax(fmax(__dsub_rn(lo[0], x), __dsub_rn(x, hi[0])), 0.0);
@@ -62,51 +79,74 @@ __device__ __forceinline__ double near2(const double lo[3], const double hi[3], 
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-// ---------------------------------------------------------------------------
-// Evaluators: what a lane does with one chunk of sources.
+// Squared distance to the farthest point of the box (BBox::far2, multipole.h:137-141).
+__device__ __forceinline__ double far2(const double lo[3], const double hi[3], double x, double y, double z) {
+  double dx = fmax(__dsub_rn(x, lo[0]), __dsub_rn(hi[0], x));
+  double dy = fmax(__dsub_rn(y, lo[1]), __dsub_rn(hi[1], y));
+  double dz = fmax(__dsub_rn(z, lo[2]), __dsub_rn(hi[2], z));
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
 
-// Split precision, up to 8 targets per lane.
+// ---------------------------------------------------------------------------
+// Evaluators: what a lane does with one chunk of sources - two per lane
+// (sources j and j + L of the chunk for lane j of a group of L lanes), whose
+// interactions with each target are independent chains.  Target slot k of
+// lane group g is target g + k * gp; lane k mod L of the group adds that
+// target's partial sums into its FP64 sum.
+
+// Split precision, up to 4 targets per lane, up to 64 per warp.
 template <bool QUAD, bool MASK>
 struct SplitEval {
-  static constexpr int TB = 8;
+  static constexpr int TB = 4;
   const WalkArgs& a;
-  double cx, cy, cz;  // reference point (target bbox centre)
+  double cx, cy, cz;  // reference point: the walk box's centre
   float eps2;
-  int L, g, j, kmax;  // lanes per group, my group, my index in it, live target slots
+  int L, gp, g, j, kmax;
   float tx[TB], ty[TB], tz[TB];
   float ax[TB], ay[TB], az[TB];
-  double ox64 = 0.0, oy64 = 0.0, oz64 = 0.0;  // FP64 sum of the target this lane owns
-  int chunks = 0;
+  double (*acc)[3];  // FP64 sums of the targets (shared memory)
+  int ntb;
+  int chunks;
 
-  __device__ SplitEval(const WalkArgs& args) : a(args) {}
+  __device__ explicit SplitEval(const WalkArgs& args) : a(args) {}
 
-  static __device__ int groups_for(int tb) { return tb <= 8 ? 1 : tb <= 16 ? 2 : 4; }
+  static __device__ int groups_for(int tb) { return tb <= 4 ? 1 : tb <= 8 ? 2 : tb <= 16 ? 4 : tb <= 32 ? 8 : 16; }
 
-  __device__ void setup(int lane, uint32_t p0, int tb) {
-    const int gp = groups_for(tb);
+  // targets: particles p0 .. p0 + tb - 1 (tb <= 64); their FP64 sums are
+  // added to sums[0 .. tb)
+  __device__ void setup(int lane, uint32_t p0, int tb, double (*sums)[3]) {
+    acc = sums;
+    ntb = tb;
+    gp = groups_for(tb);
     L = 32 / gp;
     g = lane / L;
     j = lane & (L - 1);
     kmax = (tb + gp - 1) / gp;
-    float px = 0.f, py = 0.f, pz = 0.f;
+    float p0x = 0.f, p0y = 0.f, p0z = 0.f, p1x = 0.f, p1y = 0.f, p1z = 0.f;
     if (lane < tb) {
       const double4 q = a.pm[p0 + lane];
-      px = (float)__dsub_rn(q.x, cx);
-      py = (float)__dsub_rn(q.y, cy);
-      pz = (float)__dsub_rn(q.z, cz);
+      p0x = (float)__dsub_rn(q.x, cx), p0y = (float)__dsub_rn(q.y, cy), p0z = (float)__dsub_rn(q.z, cz);
+    }
+    if (lane + 32 < tb) {
+      const double4 q = a.pm[p0 + 32 + lane];
+      p1x = (float)__dsub_rn(q.x, cx), p1y = (float)__dsub_rn(q.y, cy), p1z = (float)__dsub_rn(q.z, cz);
     }
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
-      const int src = (g + k * gp) & 31;
-      tx[k] = __shfl_sync(kFull, px, src);
-      ty[k] = __shfl_sync(kFull, py, src);
-      tz[k] = __shfl_sync(kFull, pz, src);
+      const int t = g + k * gp;  // < 64
+      const float x0 = __shfl_sync(kFull, p0x, t & 31), x1 = __shfl_sync(kFull, p1x, t & 31);
+      const float y0 = __shfl_sync(kFull, p0y, t & 31), y1 = __shfl_sync(kFull, p1y, t & 31);
+      const float z0 = __shfl_sync(kFull, p0z, t & 31), z1 = __shfl_sync(kFull, p1z, t & 31);
+      tx[k] = t < 32 ? x0 : x1;
+      ty[k] = t < 32 ? y0 : y1;
+      tz[k] = t < 32 ? z0 : z1;
       ax[k] = ay[k] = az[k] = 0.f;
     }
-    ox64 = oy64 = oz64 = 0.0;
     chunks = 0;
   }
 
+  // Reduces the FP32 partial sums over the lane group and adds them to the
+  // FP64 sums; slot k of group g belongs to lane k mod L of the group.
   __device__ void flush() {
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
@@ -117,10 +157,11 @@ struct SplitEval {
           vy += __shfl_xor_sync(kFull, vy, o);
           vz += __shfl_xor_sync(kFull, vz, o);
         }
-        if (j == k) {
-          ox64 += (double)vx;
-          oy64 += (double)vy;
-          oz64 += (double)vz;
+        const int t = g + k * gp;
+        if (j == (k & (L - 1)) && t < ntb) {
+          acc[t][0] += (double)vx;
+          acc[t][1] += (double)vy;
+          acc[t][2] += (double)vz;
         }
         ax[k] = ay[k] = az[k] = 0.f;
       }
@@ -128,16 +169,42 @@ struct SplitEval {
     chunks = 0;
   }
 
-  __device__ void tick() {
+  __device__ __forceinline__ void tick() {
     if (++chunks == kFlushChunks) flush();
   }
 
-  // accepted cells: node ids ring[(head + i) % kQueue], i < cnt
-  __device__ void cells(const uint32_t* ring, uint32_t head, int cnt) {
-    float sx = kFarAway, sy = 0.f, sz = 0.f, m = 0.f;
-    float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f;
-    if (j < cnt) {
-      const uint32_t n = ring[(head + j) & (kQueue - 1)];
+  // one source's contribution to target slot k
+  __device__ __forceinline__ void cell_one(int k, float sx, float sy, float sz, float m, const float q[6], float& rx,
+                                           float& ry, float& rz) {
+    const float dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    float ri = rsqrtf(r2);
+    if (!QUAD && MASK) ri = r2 > 0.f ? ri : 0.f;
+    const float ri2 = ri * ri;
+    const float ri3 = ri * ri2;
+    if (QUAD) {
+      const float qx = fmaf(q[0], dx, fmaf(q[3], dy, q[4] * dz));
+      const float qy = fmaf(q[3], dx, fmaf(q[1], dy, q[5] * dz));
+      const float qz = fmaf(q[4], dx, fmaf(q[5], dy, q[2] * dz));
+      const float dqd = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
+      const float ri5 = ri3 * ri2;
+      // m d / r^3 - Q d / r^5 + 2.5 (d Q d) d / r^7
+      const float c = fmaf(2.5f * dqd, ri5 * ri2, m * ri3);
+      rx = fmaf(c, dx, -ri5 * qx);
+      ry = fmaf(c, dy, -ri5 * qy);
+      rz = fmaf(c, dz, -ri5 * qz);
+    } else {
+      const float c = m * ri3;
+      rx = c * dx, ry = c * dy, rz = c * dz;
+    }
+  }
+
+  __device__ __forceinline__ void load_cell(const uint32_t* ring, uint32_t at, bool live, float& sx, float& sy,
+                                            float& sz, float& m, float q[6]) {
+    sx = kFarAway, sy = sz = m = 0.f;
+    q[0] = q[1] = q[2] = q[3] = q[4] = q[5] = 0.f;
+    if (live) {
+      const uint32_t n = ring[at & (kQueue - 1)];
       const WNode* w = a.w + n;
       const double2 cxy = *reinterpret_cast<const double2*>(&w->cx);
       const double czz = w->cz;
@@ -148,177 +215,220 @@ struct SplitEval {
       if (QUAD) {
         const float4 qa = *reinterpret_cast<const float4*>(w->q);
         const float2 qb = a.q45[n];
-        q0 = qa.x, q1 = qa.y, q2 = qa.z, q3 = qa.w, q4 = qb.x, q5 = qb.y;
+        q[0] = qa.x, q[1] = qa.y, q[2] = qa.z, q[3] = qa.w, q[4] = qb.x, q[5] = qb.y;
       }
     }
+  }
+
+  // accepted cells: node ids ring[(head + i) % kQueue], i < cnt <= 2L
+  __device__ void cells(const uint32_t* ring, uint32_t head, int cnt) {
+    float s0x, s0y, s0z, m0, q0[6], s1x, s1y, s1z, m1, q1[6];
+    load_cell(ring, head + j, j < cnt, s0x, s0y, s0z, m0, q0);
+    load_cell(ring, head + L + j, L + j < cnt, s1x, s1y, s1z, m1, q1);
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
       if (k < kmax) {
-        const float dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-        float ri = rsqrtf(r2);
-        if (!QUAD && MASK) ri = r2 > 0.f ? ri : 0.f;
-        const float ri2 = ri * ri;
-        const float ri3 = ri * ri2;
-        if (QUAD) {
-          const float qx = fmaf(q0, dx, fmaf(q3, dy, q4 * dz));
-          const float qy = fmaf(q3, dx, fmaf(q1, dy, q5 * dz));
-          const float qz = fmaf(q4, dx, fmaf(q5, dy, q2 * dz));
-          const float dqd = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
-          const float ri5 = ri3 * ri2;
-          // m d / r^3 - Q d / r^5 + 2.5 (d Q d) d / r^7
-          const float c = fmaf(2.5f * dqd, ri5 * ri2, m * ri3);
-          ax[k] = fmaf(c, dx, fmaf(-ri5, qx, ax[k]));
-          ay[k] = fmaf(c, dy, fmaf(-ri5, qy, ay[k]));
-          az[k] = fmaf(c, dz, fmaf(-ri5, qz, az[k]));
-        } else {
-          const float c = m * ri3;
-          ax[k] = fmaf(c, dx, ax[k]);
-          ay[k] = fmaf(c, dy, ay[k]);
-          az[k] = fmaf(c, dz, az[k]);
-        }
+        float ax0, ay0, az0, ax1, ay1, az1;
+        cell_one(k, s0x, s0y, s0z, m0, q0, ax0, ay0, az0);
+        cell_one(k, s1x, s1y, s1z, m1, q1, ax1, ay1, az1);
+        ax[k] += ax0 + ax1;
+        ay[k] += ay0 + ay1;
+        az[k] += az0 + az1;
       }
     }
     tick();
   }
 
-  // direct particles: particle indices ring[(head + i) % kQueue], i < cnt
-  __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
-    float sx = kFarAway, sy = 0.f, sz = 0.f, m = 0.f;
-    if (j < cnt) {
-      const double4 p = a.pm[ring[(head + j) & (kQueue - 1)]];
+  __device__ __forceinline__ void part_one(int k, float sx, float sy, float sz, float m, float& rx, float& ry,
+                                           float& rz) {
+    const float dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    float ri = rsqrtf(r2);
+    if (MASK) ri = r2 > 0.f ? ri : 0.f;
+    const float c = m * (ri * ri) * ri;
+    rx = c * dx, ry = c * dy, rz = c * dz;
+  }
+
+  __device__ __forceinline__ void load_part(const uint32_t* ring, uint32_t at, bool live, float& sx, float& sy,
+                                            float& sz, float& m) {
+    sx = kFarAway, sy = sz = m = 0.f;
+    if (live) {
+      const double4 p = a.pm[ring[at & (kQueue - 1)]];
       sx = (float)__dsub_rn(p.x, cx);
       sy = (float)__dsub_rn(p.y, cy);
       sz = (float)__dsub_rn(p.z, cz);
       m = (float)p.w;
     }
+  }
+
+  // direct particles: particle indices ring[(head + i) % kQueue], i < cnt <= 2L
+  __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
+    float s0x, s0y, s0z, m0, s1x, s1y, s1z, m1;
+    load_part(ring, head + j, j < cnt, s0x, s0y, s0z, m0);
+    load_part(ring, head + L + j, L + j < cnt, s1x, s1y, s1z, m1);
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
       if (k < kmax) {
-        const float dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-        float ri = rsqrtf(r2);
-        if (MASK) ri = r2 > 0.f ? ri : 0.f;
-        const float c = m * (ri * ri) * ri;
-        ax[k] = fmaf(c, dx, ax[k]);
-        ay[k] = fmaf(c, dy, ay[k]);
-        az[k] = fmaf(c, dz, az[k]);
+        float ax0, ay0, az0, ax1, ay1, az1;
+        part_one(k, s0x, s0y, s0z, m0, ax0, ay0, az0);
+        part_one(k, s1x, s1y, s1z, m1, ax1, ay1, az1);
+        ax[k] += ax0 + ax1;
+        ay[k] += ay0 + ay1;
+        az[k] += az0 + az1;
       }
     }
     tick();
   }
 
-  // After the walk: the owner lane of target slot j gets its FP64 sum.
-  __device__ void finish(double& rx, double& ry, double& rz) {
+  // After a walk: every target's FP64 sum is complete.
+  __device__ void finish() {
     flush();
-    rx = ox64;
-    ry = oy64;
-    rz = oz64;
+    __syncwarp();
   }
 };
 
-// Plain FP64, up to 4 targets per lane.  Absolute FP64 positions, the same
-// formula as accel_from_source with multiplications by 1/r^2 for its
-// divisions.
+// Plain FP64, up to 2 targets per lane, up to 64 per warp.  Absolute FP64
+// positions; the formula of accel_from_source with multiplications by 1/r^2
+// in place of its divisions.
 template <bool QUAD, bool MASK>
 struct F64Eval {
-  static constexpr int TB = 4;
+  static constexpr int TB = 2;
   const WalkArgs& a;
-  double cx, cy, cz;  // unused (absolute positions)
+  double cx, cy, cz;  // unused: absolute positions
   double eps2;
-  int L, g, j, kmax;
+  int L, gp, g, j, kmax;
   double tx[TB], ty[TB], tz[TB];
   double ax[TB], ay[TB], az[TB];
+  double (*acc)[3];
+  int ntb;
 
-  __device__ F64Eval(const WalkArgs& args) : a(args) {}
+  __device__ explicit F64Eval(const WalkArgs& args) : a(args) {}
 
-  static __device__ int groups_for(int tb) { return tb <= 4 ? 1 : tb <= 8 ? 2 : tb <= 16 ? 4 : 8; }
+  static __device__ int groups_for(int tb) {
+    return tb <= 2 ? 1 : tb <= 4 ? 2 : tb <= 8 ? 4 : tb <= 16 ? 8 : tb <= 32 ? 16 : 32;
+  }
 
-  __device__ void setup(int lane, uint32_t p0, int tb) {
-    const int gp = groups_for(tb);
+  __device__ void setup(int lane, uint32_t p0, int tb, double (*sums)[3]) {
+    acc = sums;
+    ntb = tb;
+    gp = groups_for(tb);
     L = 32 / gp;
     g = lane / L;
     j = lane & (L - 1);
     kmax = (tb + gp - 1) / gp;
-    double px = 0.0, py = 0.0, pz = 0.0;
+    double p0x = 0, p0y = 0, p0z = 0, p1x = 0, p1y = 0, p1z = 0;
     if (lane < tb) {
       const double4 q = a.pm[p0 + lane];
-      px = q.x, py = q.y, pz = q.z;
+      p0x = q.x, p0y = q.y, p0z = q.z;
+    }
+    if (lane + 32 < tb) {
+      const double4 q = a.pm[p0 + 32 + lane];
+      p1x = q.x, p1y = q.y, p1z = q.z;
     }
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
-      const int src = (g + k * gp) & 31;
-      tx[k] = __shfl_sync(kFull, px, src);
-      ty[k] = __shfl_sync(kFull, py, src);
-      tz[k] = __shfl_sync(kFull, pz, src);
+      const int t = g + k * gp;
+      const double x0 = __shfl_sync(kFull, p0x, t & 31), x1 = __shfl_sync(kFull, p1x, t & 31);
+      const double y0 = __shfl_sync(kFull, p0y, t & 31), y1 = __shfl_sync(kFull, p1y, t & 31);
+      const double z0 = __shfl_sync(kFull, p0z, t & 31), z1 = __shfl_sync(kFull, p1z, t & 31);
+      tx[k] = t < 32 ? x0 : x1;
+      ty[k] = t < 32 ? y0 : y1;
+      tz[k] = t < 32 ? z0 : z1;
       ax[k] = ay[k] = az[k] = 0.0;
     }
   }
 
-  __device__ void cells(const uint32_t* ring, uint32_t head, int cnt) {
-    double sx = 1.0e30, sy = 0.0, sz = 0.0, m = 0.0;
-    double q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0, q5 = 0;
-    if (j < cnt) {
-      const uint32_t n = ring[(head + j) & (kQueue - 1)];
+  __device__ __forceinline__ void cell_one(int k, double sx, double sy, double sz, double m, const double q[6],
+                                           double& rx, double& ry, double& rz) {
+    const double dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
+    const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+    double ri = rsqrt(r2);
+    if (!QUAD && MASK) ri = r2 > 0.0 ? ri : 0.0;
+    const double ri2 = ri * ri;
+    const double ri3 = ri * ri2;
+    if (QUAD) {
+      const double qx = q[0] * dx + q[3] * dy + q[4] * dz;
+      const double qy = q[3] * dx + q[1] * dy + q[5] * dz;
+      const double qz = q[4] * dx + q[5] * dy + q[2] * dz;
+      const double dqd = dx * qx + dy * qy + dz * qz;
+      const double ri5 = ri3 * ri2;
+      const double c = m * ri3 + 2.5 * dqd * (ri5 * ri2);
+      rx = c * dx - ri5 * qx;
+      ry = c * dy - ri5 * qy;
+      rz = c * dz - ri5 * qz;
+    } else {
+      const double c = m * ri3;
+      rx = c * dx, ry = c * dy, rz = c * dz;
+    }
+  }
+
+  __device__ __forceinline__ void load_cell(const uint32_t* ring, uint32_t at, bool live, double& sx, double& sy,
+                                            double& sz, double& m, double q[6]) {
+    sx = 1.0e30, sy = sz = m = 0.0;
+    q[0] = q[1] = q[2] = q[3] = q[4] = q[5] = 0.0;
+    if (live) {
+      const uint32_t n = ring[at & (kQueue - 1)];
       const double4 cm = a.mom[n];
       sx = cm.x, sy = cm.y, sz = cm.z, m = cm.w;
       if (QUAD) {
         const double* qq = a.q64 + (size_t)n * 6;
-        q0 = qq[0], q1 = qq[1], q2 = qq[2], q3 = qq[3], q4 = qq[4], q5 = qq[5];
+#pragma unroll
+        for (int t = 0; t < 6; ++t) q[t] = qq[t];
       }
     }
+  }
+
+  __device__ void cells(const uint32_t* ring, uint32_t head, int cnt) {
+    double s0x, s0y, s0z, m0, q0[6], s1x, s1y, s1z, m1, q1[6];
+    load_cell(ring, head + j, j < cnt, s0x, s0y, s0z, m0, q0);
+    load_cell(ring, head + L + j, L + j < cnt, s1x, s1y, s1z, m1, q1);
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
       if (k < kmax) {
-        const double dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
-        const double r2 = dx * dx + dy * dy + dz * dz + eps2;
-        double ri = rsqrt(r2);
-        if (!QUAD && MASK) ri = r2 > 0.0 ? ri : 0.0;
-        const double ri2 = ri * ri;
-        const double ri3 = ri * ri2;
-        if (QUAD) {
-          const double qx = q0 * dx + q3 * dy + q4 * dz;
-          const double qy = q3 * dx + q1 * dy + q5 * dz;
-          const double qz = q4 * dx + q5 * dy + q2 * dz;
-          const double dqd = dx * qx + dy * qy + dz * qz;
-          const double ri5 = ri3 * ri2;
-          const double c = m * ri3 + 2.5 * dqd * (ri5 * ri2);
-          ax[k] += c * dx - ri5 * qx;
-          ay[k] += c * dy - ri5 * qy;
-          az[k] += c * dz - ri5 * qz;
-        } else {
-          const double c = m * ri3;
-          ax[k] += c * dx;
-          ay[k] += c * dy;
-          az[k] += c * dz;
-        }
+        double ax0, ay0, az0, ax1, ay1, az1;
+        cell_one(k, s0x, s0y, s0z, m0, q0, ax0, ay0, az0);
+        cell_one(k, s1x, s1y, s1z, m1, q1, ax1, ay1, az1);
+        ax[k] += ax0 + ax1;
+        ay[k] += ay0 + ay1;
+        az[k] += az0 + az1;
       }
     }
+  }
+
+  __device__ __forceinline__ void part_one(int k, double sx, double sy, double sz, double m, double& rx, double& ry,
+                                           double& rz) {
+    const double dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
+    const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+    double ri = rsqrt(r2);
+    if (MASK) ri = r2 > 0.0 ? ri : 0.0;
+    const double c = m * (ri * ri) * ri;
+    rx = c * dx, ry = c * dy, rz = c * dz;
   }
 
   __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
-    double sx = 1.0e30, sy = 0.0, sz = 0.0, m = 0.0;
+    double s0x = 1.0e30, s0y = 0, s0z = 0, m0 = 0, s1x = 1.0e30, s1y = 0, s1z = 0, m1 = 0;
     if (j < cnt) {
       const double4 p = a.pm[ring[(head + j) & (kQueue - 1)]];
-      sx = p.x, sy = p.y, sz = p.z, m = p.w;
+      s0x = p.x, s0y = p.y, s0z = p.z, m0 = p.w;
+    }
+    if (L + j < cnt) {
+      const double4 p = a.pm[ring[(head + L + j) & (kQueue - 1)]];
+      s1x = p.x, s1y = p.y, s1z = p.z, m1 = p.w;
     }
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
       if (k < kmax) {
-        const double dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
-        const double r2 = dx * dx + dy * dy + dz * dz + eps2;
-        double ri = rsqrt(r2);
-        if (MASK) ri = r2 > 0.0 ? ri : 0.0;
-        const double c = m * (ri * ri) * ri;
-        ax[k] += c * dx;
-        ay[k] += c * dy;
-        az[k] += c * dz;
+        double ax0, ay0, az0, ax1, ay1, az1;
+        part_one(k, s0x, s0y, s0z, m0, ax0, ay0, az0);
+        part_one(k, s1x, s1y, s1z, m1, ax1, ay1, az1);
+        ax[k] += ax0 + ax1;
+        ay[k] += ay0 + ay1;
+        az[k] += az0 + az1;
       }
     }
   }
 
-  __device__ void finish(double& rx, double& ry, double& rz) {
-    rx = ry = rz = 0.0;
+  __device__ void finish() {
 #pragma unroll
     for (int k = 0; k < TB; ++k) {
       if (k < kmax) {
@@ -328,37 +438,109 @@ struct F64Eval {
           vy += __shfl_xor_sync(kFull, vy, o);
           vz += __shfl_xor_sync(kFull, vz, o);
         }
-        if (j == k) rx = vx, ry = vy, rz = vz;
+        const int t = g + k * gp;
+        if (j == (k & (L - 1)) && t < ntb) {
+          acc[t][0] += vx;
+          acc[t][1] += vy;
+          acc[t][2] += vz;
+        }
       }
     }
+    __syncwarp();
   }
 };
 
-
 // ---------------------------------------------------------------------------
-// The traversal of one target (one batch of at most 32 of its particles).
-// Returns true if the stack would overflow (the caller redoes the batch
-// popping one node at a time, which bounds the stack by 7 * depth + 1).
+// One traversal.  GROUP mode (the shared group walk): accepted -> cells,
+// rejected for the whole box -> opened, otherwise deferred to S.defer.
+// TARGET mode: accepted -> cells, otherwise opened.  The walk starts from
+// the root (nstart == 0) or from the nstart deferred nodes.  Returns 1 if
+// the stack would overflow (redo popping one node at a time, which bounds
+// it), 2 if the deferred list would overflow (GROUP mode: give up sharing).
 
+enum { kModeTarget = 0, kModeGroup = 1 };
+
+// The evaluators are reached from exactly one call site each (their bodies
+// are specialised on the live target count and would otherwise be inlined
+// many times over): the step loop below alternates between appending to
+// the queues and evaluating one queue chunk, and k_walk runs every walk of a
+// group through one call of walk_and_sum.
 template <class E>
-__device__ __forceinline__ bool walk_target(E& ev, const WalkArgs& a, WarpQueues& Q, uint32_t* stack, uint32_t root,
-                                            const double lo[3], const double hi[3], double theta2, bool dfs, int lane,
-                                            unsigned long long& ncells, unsigned long long& nparts) {
-  const int L = ev.L;
+__device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, uint32_t nstart,
+                                 const double lo[3], const double hi[3], double theta2, bool group_mode, bool dfs,
+                                 int lane, unsigned long long& ncells, unsigned long long& nparts, uint32_t& ndefer) {
+  const int C = 2 * ev.L;  // sources per evaluated chunk
   const uint32_t lt = lanemask_lt();
-  uint32_t top = 1;
-  if (lane == 0) stack[0] = root;
+  uint32_t top;
+  if (nstart == 0) {
+    if (lane == 0) S.stack[0] = root;
+    top = 1;
+  } else {
+    for (uint32_t i = lane; i < nstart; i += 32) S.stack[i] = S.defer[i];
+    top = nstart;
+  }
   __syncwarp();
   uint32_t chead = 0, phead = 0;
   int ncell = 0, npart = 0;
   ncells = nparts = 0;
-  while (top > 0) {
+  ndefer = 0;
+  // a walk pops each node at most once: more steps than nodes means a
+  // corrupt tree
+  uint32_t steps = 0;
+  const uint32_t max_steps = a.st->n_nodes + 2;
+  // particles of the leaves opened by the current step, still to enqueue
+  uint32_t ptot = 0, pbase = 0, pinc = 0, pc = 0, pfirst = 0;
+  for (;;) {
+    const bool done = top == 0 && pbase >= ptot;
+    // 1. one chunk of work: a cell chunk, a particle chunk, or enqueue
+    if (ncell >= C || (done && ncell > 0)) {
+      const int c = min(ncell, C);
+      ev.cells(S.cell, chead, c);
+      chead += c;
+      ncell -= c;
+      ncells += c;
+      continue;
+    }
+    if (npart >= C || (done && npart > 0)) {
+      const int c = min(npart, C);
+      ev.parts(S.part, phead, c);
+      phead += c;
+      npart -= c;
+      nparts += c;
+      continue;
+    }
+    if (done) break;
+    if (pbase < ptot) {  // enqueue up to 32 particles of the opened leaves
+      const uint32_t idx = pbase + lane;
+      uint32_t src = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t v = __shfl_sync(kFull, pinc, (src + step - 1) & 31);
+        if (v <= idx) src += step;
+      }
+      src = min(src, 31u);
+      const uint32_t sf = __shfl_sync(kFull, pfirst, src);
+      const uint32_t sinc = __shfl_sync(kFull, pinc, src);
+      const uint32_t spc = __shfl_sync(kFull, pc, src);
+      const uint32_t take = min(32u, ptot - pbase);
+      if ((uint32_t)lane < take) S.part[(phead + npart + lane) & (kQueue - 1)] = sf + (idx - (sinc - spc));
+      npart += take;
+      pbase += take;
+      __syncwarp();
+      continue;
+    }
+    // 2. one traversal step: pop up to 32 nodes and classify them
+    if (++steps > max_steps) {
+      if (lane == 0) atomicOr(&a.st->status, kStWalkLimit);
+      top = 0;
+      continue;
+    }
     const uint32_t n = dfs ? 1u : min(top, 32u);
     top -= n;
     const bool valid = (uint32_t)lane < n;
-    const uint32_t node = valid ? stack[top + lane] : 0u;
+    const uint32_t node = valid ? S.stack[top + lane] : 0u;
     __syncwarp();
-    bool accept = false, leaf = false;
+    bool accept = false, open = false, leaf = false;
     uint32_t first = 0, cnt = 0, info = 0;
     if (valid) {
       const WNode* w = a.w + node;
@@ -367,158 +549,204 @@ __device__ __forceinline__ bool walk_target(E& ev, const WalkArgs& a, WarpQueues
       first = u4.x;
       cnt = u4.y;
       info = u4.z;
+      leaf = info_leaf(info);
       // mac_accept_bbox: theta^2 * near^2 > edge^2 (multipole.h:151-153)
       accept = __dmul_rn(theta2, near2(lo, hi, c4.x, c4.y, c4.z)) > c4.w;
-      leaf = info_leaf(info);
+      if (!accept) {
+        // group walk: mac_reject_all, theta^2 * far^2 <= edge^2 (multipole.h:158-160)
+        open = !group_mode || __dmul_rn(theta2, far2(lo, hi, c4.x, c4.y, c4.z)) <= c4.w;
+      }
     }
     // accepted: cell queue
     const uint32_t am = __ballot_sync(kFull, accept);
-    if (accept) Q.cell[(chead + ncell + __popc(am & lt)) & (kQueue - 1)] = node;
+    if (accept) S.cell[(chead + ncell + __popc(am & lt)) & (kQueue - 1)] = node;
     ncell += __popc(am);
+    if (group_mode) {  // neither: deferred to the targets
+      const bool defer = valid && !accept && !open;
+      const uint32_t dm = __ballot_sync(kFull, defer);
+      if (ndefer + __popc(dm) > (uint32_t)kDeferCap) return 2;
+      if (defer) S.defer[ndefer + __popc(dm & lt)] = node;
+      ndefer += __popc(dm);
+    }
     // opened interior nodes: push the children
-    const uint32_t nch = (valid && !accept && !leaf) ? info_nchild(info) : 0u;
+    const uint32_t nch = (open && !leaf) ? info_nchild(info) : 0u;
     const uint32_t cinc = warp_incl_scan_u32(nch, lane);
     const uint32_t ctot = __shfl_sync(kFull, cinc, 31);
-    if (top + ctot > a.stack_cap) return true;
-    for (uint32_t k = 0; k < nch; ++k) stack[top + cinc - nch + k] = first + k;
+    if (top + ctot > (uint32_t)kStackCap) return 1;
+    for (uint32_t k = 0; k < nch; ++k) S.stack[top + cinc - nch + k] = first + k;
     top += ctot;
-    // opened leaves: their particles
-    const uint32_t pc = (valid && !accept && leaf) ? cnt : 0u;
-    const uint32_t pinc = warp_incl_scan_u32(pc, lane);
-    const uint32_t ptot = __shfl_sync(kFull, pinc, 31);
+    // opened leaves: their particles, enqueued by the next iterations
+    pc = (open && leaf) ? cnt : 0u;
+    pinc = warp_incl_scan_u32(pc, lane);
+    ptot = __shfl_sync(kFull, pinc, 31);
+    pbase = 0;
+    pfirst = first;
     __syncwarp();
-    while (ncell >= L) {
-      ev.cells(Q.cell, chead, L);
-      chead += L;
-      ncell -= L;
-      ncells += L;
-    }
-    for (uint32_t base = 0; base < ptot; base += 32) {
-      const uint32_t idx = base + lane;
-      uint32_t src = 0;
-#pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const uint32_t v = __shfl_sync(kFull, pinc, (src + step - 1) & 31);
-        if (v <= idx) src += step;
-      }
-      src = min(src, 31u);
-      const uint32_t sf = __shfl_sync(kFull, first, src);
-      const uint32_t sinc = __shfl_sync(kFull, pinc, src);
-      const uint32_t spc = __shfl_sync(kFull, pc, src);
-      const uint32_t take = min(32u, ptot - base);
-      if ((uint32_t)lane < take) Q.part[(phead + npart + lane) & (kQueue - 1)] = sf + (idx - (sinc - spc));
-      npart += take;
-      __syncwarp();
-      while (npart >= L) {
-        ev.parts(Q.part, phead, L);
-        phead += L;
-        npart -= L;
-        nparts += L;
-      }
-    }
-    __syncwarp();
-  }
-  if (ncell > 0) {
-    ev.cells(Q.cell, chead, ncell);
-    ncells += ncell;
-  }
-  if (npart > 0) {
-    ev.parts(Q.part, phead, npart);
-    nparts += npart;
   }
   __syncwarp();
-  return false;
+  return 0;
 }
 
+// Bounding box of particles [b, b + T) (BBox::add, multipole.h:121-128).
+__device__ __forceinline__ void particle_box(const double4* pm, uint32_t b, uint32_t T, int lane, double lo[3],
+                                             double hi[3]) {
+  lo[0] = lo[1] = lo[2] = INFINITY;
+  hi[0] = hi[1] = hi[2] = -INFINITY;
+  for (uint32_t i = lane; i < T; i += 32) {
+    const double4 q = pm[b + i];
+    lo[0] = fmin(lo[0], q.x), hi[0] = fmax(hi[0], q.x);
+    lo[1] = fmin(lo[1], q.y), hi[1] = fmax(hi[1], q.y);
+    lo[2] = fmin(lo[2], q.z), hi[2] = fmax(hi[2], q.z);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(kFull, hi[d], o));
+    }
+  }
+}
+
+// Evaluates the walk of the targets [p0, p0 + tb) (tb <= 64) into the FP64
+// sums[0 .. tb), zeroed first (and again if the walk is redone).
+template <class E>
+__device__ __forceinline__ int walk_and_sum(E& ev, const WalkArgs& a, WarpSmem& S, double (*sums)[3], uint32_t root,
+                                            uint32_t nstart, const double lo[3], const double hi[3], double theta2,
+                                            bool group_mode, uint32_t p0, int tb, int lane, unsigned long long& n_pp,
+                                            unsigned long long& n_pc, bool quad, uint32_t& ndefer) {
+  unsigned long long nc = 0, np = 0;
+  int r = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    for (int t = lane; t < tb; t += 32) sums[t][0] = sums[t][1] = sums[t][2] = 0.0;
+    __syncwarp();
+    ev.setup(lane, p0, tb, sums);
+    r = walk(ev, a, S, root, nstart, lo, hi, theta2, group_mode, attempt == 1, lane, nc, np, ndefer);
+    if (r != 1) break;
+  }
+  if (r == 2) return 2;  // GROUP mode only: the caller discards this walk
+  ev.finish();
+  if (quad) {
+    n_pc += nc * (unsigned long long)tb;
+    n_pp += np * (unsigned long long)tb;
+  } else {
+    n_pp += (nc + np) * (unsigned long long)tb;
+  }
+  return 0;
+}
+
+// on_result(particle, G * acc) (grouped_ttg.h:281-283), then kick_one /
+// drift_one (integrate.h:15-16), for particles p0 .. p0 + n - 1 whose FP64
+// sums are in sums[0 .. n).
+__device__ __forceinline__ void kick_drift(const WalkArgs& a, const SysParam& sp, const double (*sums)[3], uint32_t p0,
+                                           uint32_t n, int lane) {
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t p = p0 + i;
+    const double gx = __dmul_rn(sp.G, sums[i][0]), gy = __dmul_rn(sp.G, sums[i][1]), gz = __dmul_rn(sp.G, sums[i][2]);
+    if (a.accel) {
+      a.accel[3 * (size_t)p + 0] = gx;
+      a.accel[3 * (size_t)p + 1] = gy;
+      a.accel[3 * (size_t)p + 2] = gz;
+    }
+    Particle P = a.staged[p];
+    P.vel[0] = __dadd_rn(P.vel[0], __dmul_rn(sp.kick_dt, gx));
+    P.vel[1] = __dadd_rn(P.vel[1], __dmul_rn(sp.kick_dt, gy));
+    P.vel[2] = __dadd_rn(P.vel[2], __dmul_rn(sp.kick_dt, gz));
+    if (sp.drift_dt != 0.0) {
+      P.pos[0] = __dadd_rn(P.pos[0], __dmul_rn(sp.drift_dt, P.vel[0]));
+      P.pos[1] = __dadd_rn(P.pos[1], __dmul_rn(sp.drift_dt, P.vel[1]));
+      P.pos[2] = __dadd_rn(P.pos[2], __dmul_rn(sp.drift_dt, P.vel[2]));
+    }
+    a.out[p] = P;
+  }
+  __syncwarp();
+}
+
+// One warp per walk group.  The walks of a group - its shared group walk,
+// then one per target (one per kGroupMax particles of a large leaf target) -
+// run as consecutive jobs through a single walk_and_sum call.
 template <class E, bool QUAD>
 __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
-  __shared__ WarpQueues sq[kWalkWarps];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  WarpQueues& Q = sq[warp];
-  uint32_t* stack = a.stack + (size_t)(blockIdx.x * kWalkWarps + warp) * a.stack_cap;
+  WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
   if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;  // the build failed: touch nothing
-  const uint32_t ntg = a.st->n_targets;
+  const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
   unsigned long long n_pp = 0, n_pc = 0;
   E ev(a);
   for (;;) {
-    uint32_t ti = 0;
-    if (lane == 0) ti = atomicAdd(&a.st->walk_next, 1u);
-    ti = __shfl_sync(kFull, ti, 0);
-    if (ti >= ntg) break;
-    const uint32_t tnode = a.targets[ti];
-    const uint32_t tb = a.nbegin[tnode], T = a.ncount[tnode];
+    uint32_t gi = 0;
+    if (lane == 0) gi = atomicAdd(&a.st->walk_next, 1u);
+    gi = __shfl_sync(kFull, gi, 0);
+    if (gi >= ngroups) break;
+    const uint32_t gnode = a.groups[gi];
+    const uint32_t gb = a.nbegin[gnode], gn = a.ncount[gnode];
     uint32_t s = 0;
-    if (a.nsys > 1) {  // the system holding particle tb
+    if (a.nsys > 1) {  // the system holding particle gb
       uint32_t lo = 0, hi = (uint32_t)a.nsys;
       while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (a.sys[mid].begin <= tb) lo = mid;
+        if (a.sys[mid].begin <= gb) lo = mid;
         else hi = mid;
       }
       s = lo;
     }
-    const SysDev& sd = a.sys[s];
+    const uint32_t root = a.sys[s].root;
     const SysParam& sp = a.prm[s];
-    // BBox of the target's particles (multipole.h:115-129)
-    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t i = lane; i < T; i += 32) {
-      const double4 q = a.pm[tb + i];
-      lo[0] = fmin(lo[0], q.x), hi[0] = fmax(hi[0], q.x);
-      lo[1] = fmin(lo[1], q.y), hi[1] = fmax(hi[1], q.y);
-      lo[2] = fmin(lo[2], q.z), hi[2] = fmax(hi[2], q.z);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], o));
-        hi[d] = fmax(hi[d], __shfl_xor_sync(kFull, hi[d], o));
-      }
-    }
-    ev.cx = 0.5 * (lo[0] + hi[0]);
-    ev.cy = 0.5 * (lo[1] + hi[1]);
-    ev.cz = 0.5 * (lo[2] + hi[2]);
+    const double theta2 = sp.theta2;
     ev.eps2 = sp.eps2;
-    const double theta2 = sp.theta2, G = sp.G, kick = sp.kick_dt, drift = sp.drift_dt;
-    for (uint32_t b0 = 0; b0 < T; b0 += 32) {
-      const int tbn = (int)min(32u, T - b0);
-      unsigned long long nc = 0, np = 0;
-      for (int attempt = 0; attempt < 2; ++attempt) {
-        ev.setup(lane, tb + b0, tbn);
-        if (!walk_target(ev, a, Q, stack, sd.root, lo, hi, theta2, attempt == 1, lane, nc, np)) break;
-      }
-      double rx, ry, rz;
-      ev.finish(rx, ry, rz);
-      if (QUAD) {
-        n_pc += nc * (unsigned long long)tbn;
-        n_pp += np * (unsigned long long)tbn;
-      } else {
-        n_pp += (nc + np) * (unsigned long long)tbn;
-      }
-      const int gp = 32 / ev.L;
-      const int tl = ev.g + ev.j * gp;
-      if (ev.j < ev.kmax && tl < tbn) {
-        const uint32_t p = tb + b0 + (uint32_t)tl;
-        // on_result(particle, G * acc) (grouped_ttg.h:281-283), then
-        // kick_one / drift_one (integrate.h:15-16)
-        const double gx = __dmul_rn(G, rx), gy = __dmul_rn(G, ry), gz = __dmul_rn(G, rz);
-        if (a.accel) {
-          a.accel[3 * (size_t)p + 0] = gx;
-          a.accel[3 * (size_t)p + 1] = gy;
-          a.accel[3 * (size_t)p + 2] = gz;
+    uint32_t ti = a.group_first[gi];
+    const bool single = ti < ntargets && a.targets[ti] == gnode;  // the group is its own target
+    bool group_job = !single, shared = false;
+    uint32_t ndefer = 0, tb = gb, T = gn, b0 = 0;
+    double lo[3], hi[3];
+    particle_box(a.pm, gb, gn, lane, lo, hi);
+    for (;;) {
+      // -- the next job: the group walk, or (a batch of) the next target
+      if (!group_job) {
+        if (b0 == 0) {
+          if (!single) {
+            if (ti >= ntargets) break;
+            const uint32_t tnode = a.targets[ti];
+            tb = a.nbegin[tnode];
+            T = a.ncount[tnode];
+            if (tb >= gb + gn || (shared && ndefer == 0)) break;  // past the group, or nothing deferred
+            particle_box(a.pm, tb, T, lane, lo, hi);
+          }
         }
-        Particle P = a.staged[p];
-        P.vel[0] = __dadd_rn(P.vel[0], __dmul_rn(kick, gx));
-        P.vel[1] = __dadd_rn(P.vel[1], __dmul_rn(kick, gy));
-        P.vel[2] = __dadd_rn(P.vel[2], __dmul_rn(kick, gz));
-        if (drift != 0.0) {
-          P.pos[0] = __dadd_rn(P.pos[0], __dmul_rn(drift, P.vel[0]));
-          P.pos[1] = __dadd_rn(P.pos[1], __dmul_rn(drift, P.vel[1]));
-          P.pos[2] = __dadd_rn(P.pos[2], __dmul_rn(drift, P.vel[2]));
-        }
-        a.out[p] = P;
       }
+      const uint32_t p0 = group_job ? gb : tb + b0;
+      const int nt = (int)(group_job ? gn : min((uint32_t)kGroupMax, T - b0));
+      double(*sums)[3] = (group_job || single) ? S.acc : S.tacc;
+      ev.cx = 0.5 * (lo[0] + hi[0]), ev.cy = 0.5 * (lo[1] + hi[1]), ev.cz = 0.5 * (lo[2] + hi[2]);
+      uint32_t nd = 0;
+      const int r = walk_and_sum(ev, a, S, sums, root, (!group_job && shared) ? ndefer : 0u, lo, hi, theta2, group_job,
+                                 p0, nt, lane, n_pp, n_pc, QUAD, nd);
+      // -- what the job leaves behind
+      if (group_job) {
+        group_job = false;
+        shared = r == 0;
+        ndefer = nd;
+        if (!shared) {  // too many deferred nodes: every target walks from the root
+          for (uint32_t i = lane; i < gn; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
+          __syncwarp();
+        }
+        continue;
+      }
+      if (single) {  // a batch of a large target is written out right away
+        kick_drift(a, sp, S.acc, p0, (uint32_t)nt, lane);
+        b0 += kGroupMax;
+        if (b0 >= T) break;
+        continue;
+      }
+      for (int i = lane; i < nt; i += 32) {  // the target's own part onto the group's shared part
+        double* d = S.acc[p0 - gb + (uint32_t)i];
+        d[0] += S.tacc[i][0], d[1] += S.tacc[i][1], d[2] += S.tacc[i][2];
+      }
+      __syncwarp();
+      ++ti;
     }
+    if (!single) kick_drift(a, sp, S.acc, gb, gn, lane);
   }
   if (lane == 0) {
     atomicAdd(&a.st->pp, n_pp);
@@ -528,7 +756,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
 
 template <class E, bool QUAD>
 static void launch_one(const WalkArgs& a, int grid, cudaStream_t s) {
-  k_walk<E, QUAD><<<grid, kWalkThreads, 0, s>>>(a);
+  k_walk<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
 }
 
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s) {
@@ -543,18 +771,28 @@ void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int gri
 
 template <class E, bool QUAD>
 static int occ() {
+  cudaFuncSetAttribute(k_walk<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<E, QUAD>, kWalkThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<E, QUAD>, kWalkThreads, kWalkSmem);
   return b > 0 ? b : 1;
 }
 
-int walk_blocks_per_sm(int precision, bool quad, bool mask) {
+static int walk_blocks_per_sm_query(int precision, bool quad, bool mask) {
   if (precision == 0) {
     if (quad) return mask ? occ<SplitEval<true, true>, true>() : occ<SplitEval<true, false>, true>();
     return mask ? occ<SplitEval<false, true>, false>() : occ<SplitEval<false, false>, false>();
   }
   if (quad) return mask ? occ<F64Eval<true, true>, true>() : occ<F64Eval<true, false>, true>();
   return mask ? occ<F64Eval<false, true>, false>() : occ<F64Eval<false, false>, false>();
+}
+
+// Cached: queried (and the kernels' shared-memory limit raised) once per
+// variant, before any stream capture uses it.
+int walk_blocks_per_sm(int precision, bool quad, bool mask) {
+  static int cache[2][2][2] = {};
+  int& v = cache[precision != 0][quad][mask];
+  if (v == 0) v = walk_blocks_per_sm_query(precision, quad, mask);
+  return v;
 }
 
 int walk_threads() { return kWalkThreads; }
@@ -587,7 +825,11 @@ void launch_integrate(Particle* p, const double* accel, uint32_t n, const SysDev
 }
 
 __global__ void k_eval_done(DevState* st) {
-  if (st->status == 0u) st->evals_ok += 1u;
+  if (st->status == 0u) {
+    st->evals_ok += 1u;
+    st->pp_total += st->pp;
+    st->pc_total += st->pc;
+  }
 }
 
 void launch_eval_done(DevState* st, cudaStream_t s) { k_eval_done<<<1, 1, 0, s>>>(st); }

@@ -69,19 +69,25 @@ typedef struct bhg_force_params {
   int precision;
 } bhg_force_params;
 
-/* Per-phase device times of the last step (CUDA events on the context's
- * stream), and interaction counts of the last walk. */
+/* Device time per phase, summed over the evaluations since the last reset
+ * (CUDA events recorded around each phase on the context's stream), and the
+ * interaction counts of those evaluations. */
 typedef struct bhg_stats {
-  double build_ms;     /* bounds, keys, sort, gather, topology */
+  double pre_ms;       /* bounds, domain, Morton keys, digit histograms */
+  double sort_ms;      /* the radix-sort passes */
+  double tree_ms;      /* gather into Morton order + octree topology */
   double multipole_ms; /* upward pass */
-  double walk_ms;      /* force walk (+ fused kick/drift) */
-  double sort_ms;      /* the radix sort alone (inside build_ms) */
+  double targets_ms;   /* walk targets */
+  double walk_ms;      /* force walk with fused kick/drift */
+  double last_walk_ms; /* the most recent walk alone */
   uint64_t pp;         /* particle-particle interactions (monopole cells included in no-quad mode) */
   uint64_t pc;         /* particle-cell quadrupole interactions */
-  uint32_t nodes;      /* octree nodes */
-  uint32_t targets;    /* walk targets */
-  uint32_t depth;      /* deepest level + 1 */
+  uint32_t evals;      /* walks timed */
+  uint32_t nodes;      /* octree nodes of the last build */
+  uint32_t targets;    /* walk targets of the last walk */
+  uint32_t depth;      /* levels of the last build */
   uint32_t sort_passes;
+  uint32_t kernels_per_eval; /* kernel launches of one evaluation (bhg_step) */
 } bhg_stats;
 
 /* ---- lifetime ---------------------------------------------------------- */
@@ -153,7 +159,8 @@ int bhg_run_schedule(bhg_context* ctx, const bhg_force_params* fp, unsigned max_
 int bhg_set_system_params(bhg_context* ctx, const double* theta, const double* eps2, const double* kick_dt,
                           const double* drift_dt);
 
-int bhg_get_stats(bhg_context* ctx, bhg_stats* out);
+/* Blocks.  reset != 0 starts new sums after reading. */
+int bhg_get_stats(bhg_context* ctx, bhg_stats* out, int reset);
 /* Device-side status bits of the last step (0 = fine); blocks. */
 int bhg_device_status(bhg_context* ctx, uint32_t* status);
 

@@ -65,6 +65,7 @@ def test_walk_matches_oracle(gpu, oracle, name, make, max_leaf, gs, ts, theta, e
         tg = oracle.targets(t, ts, gs)
         racc, counts = oracle.walk(t, tg, soa(mp), [Params(theta, eps2, 1.0, int(quad))] * len(tg))
         gpu.upload(parts)
+        gpu.stats(reset=True)
         gpu.build_tree(max_leaf, gs)
         gpu.compute_multipoles()
         acc = gpu.walk_forces(bhg.Context.params(theta, eps2, 1.0, quad, precision), ts)
