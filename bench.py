@@ -314,6 +314,20 @@ def main():
                "d2h_bytes_per_step": w["n"] * 64, "ms_per_step": ems / args.steps,
                "path": "bhg_upload (pinned host) + bhg_run_schedule + bhg_download"}
 
+    # accuracy: rms and 99th-percentile relative force error of this walk
+    # against an FP64 direct sum on 4,096 sampled particles
+    acc_err = None
+    if rank == 0:
+        ctx.build_tree(w["max_leaf"], w["group"])
+        ctx.compute_multipoles()
+        acc = ctx.walk_forces(fp, w["target"])  # kick = drift = 0: positions unchanged
+        idx = np.sort(np.random.default_rng(12345).choice(w["n"], size=min(4096, w["n"]), replace=False))
+        ref = ctx.direct_sum(idx.astype(np.uint32), w["eps"] ** 2)
+        rel = np.linalg.norm(acc[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        acc_err = {"vs": "FP64 direct sum (GPU, brute_force.h semantics) on 4096 sampled particles",
+                   "rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99)),
+                   "global": float(np.sqrt(np.sum((acc[idx] - ref) ** 2) / np.sum(ref ** 2)))}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -352,6 +366,7 @@ def main():
                                                               "targets_ms", "walk_ms")},
             "interactions_per_particle": {"pp": st["pp"] / (w["n"] * evals), "pc": st["pc"] / (w["n"] * evals)},
             "clocks": clk.summary(),
+            "force_error": acc_err,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }

@@ -195,8 +195,8 @@ class Reference:
     def available(cls) -> bool:
         return os.path.exists(cls.PATH)
 
-    def __init__(self):
-        L = self.lib = C.CDLL(self.PATH)
+    def __init__(self, path=None):
+        L = self.lib = C.CDLL(path or self.PATH)
         vp, sz, u32, f64 = C.c_void_p, C.c_size_t, C.c_uint32, C.c_double
         L.bhref_build.argtypes = [vp, sz, C.c_uint, u32]
         L.bhref_build.restype = vp

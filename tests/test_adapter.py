@@ -1,0 +1,56 @@
+"""The C++ drop-in for bh::step_particles (amt-bh-benchmark_b200/include/
+bhg_step_particles.hpp): it compiles against the reference's own types (CPU,
+where the reference tree exists) and, on the GPU, runs the reference's
+leapfrog schedule to the oracle's result."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "amt-bh-benchmark_b200")
+SRC = os.path.join(ROOT, "tests", "cpp", "adapter_main.cc")
+REF_SRC = "/root/reference/ttg-parsec/src"
+INC = ["-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(PKG, "include")]
+LINK = ["-L" + PKG, "-lbhg", "-Wl,-rpath," + PKG]
+
+
+def compile_adapter(out, reference_types=False):
+    cmd = ["g++", "-std=c++20", "-O2", *INC, SRC, "-o", out, *LINK, "-pthread"]
+    if reference_types:
+        cmd[3:3] = ["-DBHG_WITH_REFERENCE_TYPES", "-I" + os.path.join(ROOT, "oracle", "ttg_shim"), "-I" + REF_SRC]
+        cmd.insert(-4, os.path.join(REF_SRC, "tree.cc"))
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference sources not present")
+def test_adapter_compiles_against_reference_types(tmp_path):
+    compile_adapter(str(tmp_path / "adapter_ref"), reference_types=True)
+
+
+def test_adapter_compiles_against_layout_twins(tmp_path):
+    compile_adapter(str(tmp_path / "adapter_local"))
+
+
+@pytest.mark.gpu
+def test_adapter_schedule_matches_oracle(tmp_path, oracle):
+    import bhg
+
+    parts, _ = bhg.plummer(8192, 41)
+    exe = str(tmp_path / "adapter")
+    compile_adapter(exe)
+    src, dst = tmp_path / "in.bin", tmp_path / "out.bin"
+    parts.tofile(src)
+    dt, steps = 1 / 128, 3
+    r = subprocess.run([exe, str(src), str(dst), "0.5", "0.01", repr(dt), str(steps), "1"], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = np.fromfile(dst, dtype=bhg.PARTICLE)
+    ref = parts
+    for k, d in [(dt / 2, dt)] + [(dt, dt)] * (steps - 1) + [(dt / 2, 0.0)]:
+        ref, _, _ = oracle.step(ref, theta=0.5, eps2=1e-4, max_leaf=16, group_size=256, target_size=16,
+                                kick_dt=k, drift_dt=d)
+    assert np.array_equal(out["id"], ref["id"])
+    assert np.max(np.abs(out["pos"] - ref["pos"])) < 1e-10

@@ -191,3 +191,12 @@ def test_node_overflow_regrows(gpu, oracle):
     out = gpu.download()
     ref, _, _ = oracle.step(parts, theta=0.5, eps2=1e-8, max_leaf=1, group_size=64, target_size=0)
     assert np.array_equal(out["id"], ref["id"])
+
+
+def test_hbm_budget_is_enforced():
+    # a budget too small for the particle arrays: a clean BHG_ENOMEM, no fault
+    ctx = bhg.Context(device=0, hbm_budget=1 << 20)
+    with pytest.raises(bhg.BhgError) as e:
+        ctx.upload(cube(100000, 1))
+    assert e.value.code == bhg.ENOMEM
+    ctx.close()
