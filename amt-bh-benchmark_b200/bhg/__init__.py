@@ -33,7 +33,8 @@ EXPORTED = (
     "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_build_tree",
     "bhg_compute_multipoles", "bhg_walk_forces", "bhg_integrate", "bhg_step", "bhg_step_systems",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
-    "bhg_direct_sum", "bhg_energy", "bhg_ic_plummer", "bhg_write_csv", "bhg_measure_fp32_peak",
+    "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
+    "bhg_measure_fp32_peak",
 )
 
 
@@ -101,6 +102,7 @@ def lib() -> C.CDLL:
         "bhg_debug_export": ([vp, i32, vp, sz, C.POINTER(sz)], i32),
         "bhg_direct_sum": ([vp, i32, vp, sz, f64, f64, vp], i32),
         "bhg_energy": ([vp, i32, f64, C.POINTER(f64), C.POINTER(f64)], i32),
+        "bhg_energy_noalloc": ([vp, sz, f64, vp, vp], i32),
         "bhg_ic_plummer": ([vp, sz, f64, f64, vp, vp, u32, u64], u64),
         "bhg_write_csv": ([C.c_char_p, vp, sz], i32),
         "bhg_measure_fp32_peak": ([i32, C.POINTER(f64)], i32),

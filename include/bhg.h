@@ -187,6 +187,20 @@ int bhg_direct_sum(bhg_context* ctx, int sys, const uint32_t* idx, size_t ns, do
  * unsoftened and O(N^2)) of system `sys` on the GPU.  Blocks. */
 int bhg_energy(bhg_context* ctx, int sys, double G, double* kinetic, double* potential);
 
+/* The energies of bhg_energy for callers that cannot allocate GPU memory
+ * (a host program whose memory pool already owns the device, or a loop that
+ * cannot afford the device-wide synchronisation of cudaFree).  No counterpart
+ * in the reference.  particles: n records in device memory of the current
+ * device; result: 2 doubles in device memory, written with (kinetic,
+ * potential).  Allocates nothing: the per-block partial sums live in a fixed
+ * 16 KB array in the library's device memory, so n is at most 262,144 (larger
+ * n returns BHG_EINVAL).  Asynchronous on `stream` (a cudaStream_t; NULL =
+ * the default stream).  The first call on a device looks up that array's
+ * device address (make it before any stream capture).  Every call shares the
+ * array: calls that overlap on the GPU race and must be serialised (one
+ * stream, or events between streams). */
+int bhg_energy_noalloc(const bh_particle64* particles, size_t n, double G, double* result, void* stream);
+
 /* ---- workload generators (synthetic initial conditions) --------------------------- */
 
 /* Plummer sphere by Aarseth-Henon-Wielen sampling (G = 1): n particles of
