@@ -310,3 +310,13 @@ def step_particles(particles, theta, eps2, G=1.0, use_quadrupole=True, max_leaf=
     fp = Context.params(theta, eps2, G, use_quadrupole, precision)
     ctx.step(fp, max_leaf, group_size, target_size, kick_dt, drift_dt)
     return ctx.download()
+
+
+def ensemble(nsys=512, seed=3, nmin=1024, nmax=262144):
+    """Independent Plummer systems (M = a = 1 each) with N log-uniform in
+    [nmin, nmax]: N_s = round(exp(U(ln nmin, ln nmax))) and per-system seeds,
+    both from numpy's PCG64 stream `seed`.  Returns a list of particle arrays."""
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsys))).astype(np.int64)
+    seeds = rng.integers(1, 2**63 - 1, nsys)
+    return [plummer(int(n), int(sd))[0] for n, sd in zip(ns, seeds)]

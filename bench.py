@@ -1,21 +1,33 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 Barnes-Hut hot path (one JSON line on rank 0).
 
-Workload (default): the single-system N = 4,194,304 Plummer sphere (seed 2,
-G = M = a = 1, theta 0.5, eps 0.005, monopole + quadrupole, max_leaf 16,
-target 16, group 256), advanced by the reference's leapfrog schedule for 8
-KDK steps of dt = 1/256 (main.cc:199-246: 9 force evaluations).  One bench
-step = that whole 8-step sequence over the GPU-resident particles; the
-metric is particle-steps/s = N * 8 * steps / time.  Other workloads:
---workload plummer-65k (N = 65,536, seed 1, eps 0.01, dt 1/128, 16 steps).
+Default workload: one Plummer sphere, N = 4,194,304
+(seed 2, G = M = a = 1), theta 0.5, eps 0.005, monopole + quadrupole,
+max_leaf 16, target 16, group 256, advanced by the reference's leapfrog
+schedule for 8 KDK steps of dt = 1/256 (main.cc:199-246: 9 force
+evaluations).  One bench step = that whole 8-step sequence over the
+GPU-resident particles; metric particle-steps/s = N * 8 * steps / time.
+
+Other workloads (--workload):
+  plummer-65k   configs[0]: N = 65,536, seed 1, eps 0.01, dt 1/128, 16 steps
+  merger-16m    configs[2]: two Plummer spheres of 8,388,608 (a = 1 and 0.5,
+                centres x = -5 / +5, approaching at 0.3), theta 0.6,
+                eps 0.002, dt 1/256, 8 steps
+  ensemble-512  configs[3]: 512 independent Plummer systems, N log-uniform in
+                [1,024, 262,144] (seed 3), eps 0.01, dt 1/128; one bench step
+                = one lockstep KDK evaluation of every system, batched in one
+                segmented key space, split precision, leaf/target sizes from
+                the autotuner; also times the plain FP64 path looping over
+                the systems one at a time (the north-star comparison)
+  plummer-1m    a smaller case of configs[1] for profiler captures
 
 --impl reference times the reference's own CPU implementation of the path
 (oracle/_ref/ref_bench: the unmodified reference sources with a thread-pool
 stand-in for TTG) on all host cores, on the same workload and metric.
 
 Multi-GPU: one process per GPU, each an independent replica of the workload
-(a Barnes-Hut system does not shard here; no collective on the data path);
-value = particle-steps of all ranks / max over ranks of the device time.
+(a system never spans GPUs; no collective on the data path); value =
+particle-steps of all ranks / max over ranks of the device time.
 """
 import argparse
 import json
@@ -32,13 +44,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "amt-bh-benchmark_b200"))
 
 WORKLOADS = {
-    "plummer-4m": dict(n=4194304, seed=2, theta=0.5, eps=0.005, max_leaf=16, target=16, group=256,
+    "plummer-4m": dict(kind="single", n=4194304, seed=2, theta=0.5, eps=0.005, max_leaf=16, target=16, group=256,
                        dt=1.0 / 256, steps=8),
-    "plummer-65k": dict(n=65536, seed=1, theta=0.5, eps=0.01, max_leaf=16, target=16, group=256,
+    "plummer-65k": dict(kind="single", n=65536, seed=1, theta=0.5, eps=0.01, max_leaf=16, target=16, group=256,
                         dt=1.0 / 128, steps=16),
-    # a smaller case of the 4M workload's parameters, for profiler captures
-    "plummer-1m": dict(n=1048576, seed=2, theta=0.5, eps=0.005, max_leaf=16, target=16, group=256,
+    "plummer-1m": dict(kind="single", n=1048576, seed=2, theta=0.5, eps=0.005, max_leaf=16, target=16, group=256,
                        dt=1.0 / 256, steps=1),
+    "merger-16m": dict(kind="merger", n=2 * 8388608, seed=4, theta=0.6, eps=0.002, max_leaf=16, target=16,
+                       group=256, dt=1.0 / 256, steps=8),
+    "ensemble-512": dict(kind="ensemble", nsys=512, seed=3, theta=0.5, eps=0.01, max_leaf=16, target=16, group=256,
+                         dt=1.0 / 128, steps=32),
 }
 METRIC = "particle-steps/s"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -56,7 +71,18 @@ def parse():
     ap.add_argument("--precision", default="split", choices=["split", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="ensemble: skip the one-at-a-time FP64 path")
     return ap.parse_args()
+
+
+def make_particles(w, rank=0):
+    import bhg
+
+    if w["kind"] == "single":
+        return bhg.plummer(w["n"], w["seed"] + rank)[0]
+    if w["kind"] == "merger":
+        return bhg.merger(w["n"] // 2, w["seed"] + rank)
+    return bhg.ensemble(w["nsys"], w["seed"] + rank)
 
 
 # ---------------------------------------------------------------------------- clocks
@@ -130,22 +156,21 @@ def ref_binary():
     return v3 if os.path.exists(v3) else None
 
 
-def run_ref(parts, w, evals, threads=None):
-    """Times `evals` evaluations of the reference schedule; returns eval ms list."""
+def run_ref(parts, w, evals, leaf=None):
+    """Times `evals` evaluations of the reference schedule; returns (eval ms list, threads)."""
     exe = ref_binary()
     if exe is None:
         raise FileNotFoundError("oracle/_ref/ref_bench is not built")
     with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
         parts.tofile(f)
         path = f.name
-    env = dict(os.environ)
-    if threads:
-        env["TTG_NUM_THREADS"] = str(threads)
+    leaf = leaf or w["max_leaf"]
     try:
         cmd = [exe, "--particles", path, "--steps", str(w["steps"]), "--evals", str(evals), "--dt", repr(w["dt"]),
-               "--theta", repr(w["theta"]), "--eps", repr(w["eps"]), "--max-leaf", str(w["max_leaf"]),
-               "--target-size", str(w["target"]), "--group-size", str(w["group"])]
-        out = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env).stdout
+               "--theta", repr(w["theta"]), "--eps", repr(w["eps"]), "--max-leaf", str(leaf),
+               "--target-size", str(w["target"] if leaf == w["max_leaf"] else leaf),
+               "--group-size", str(w["group"])]
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
     finally:
         os.unlink(path)
     rec = json.loads(out.strip().splitlines()[-1])
@@ -153,22 +178,23 @@ def run_ref(parts, w, evals, threads=None):
 
 
 def cpu_sample(w, budget_s=20.0):
-    """A bounded sample of the workload on the reference: the full system if one
-    evaluation fits the budget, else the largest power-of-two Plummer sphere of
-    the same parameters that does.  Returns (n, per-eval ms list, threads)."""
+    """A bounded sample of a single-system workload on the reference: the full
+    system if one evaluation fits the budget, else the largest power-of-two
+    system of the same kind and parameters that does.  Returns (n, eval ms, threads)."""
     import bhg
 
+    def gen(n):
+        return bhg.merger(n // 2, w["seed"]) if w["kind"] == "merger" else bhg.plummer(n, w["seed"])[0]
+
     n_probe = min(w["n"], 65536)
-    parts, _ = bhg.plummer(n_probe, w["seed"])
-    ms, threads = run_ref(parts, w, 2)
+    ms, threads = run_ref(gen(n_probe), w, 2)
     per = ms[-1] / n_probe  # ms per particle per evaluation
     n = n_probe
     while n * 2 <= w["n"] and per * (n * 2) * 1.15 * 2 / 1000.0 < budget_s:
         n *= 2
         per *= 1.1  # the walk cost per particle grows with log N
     if n != n_probe:
-        parts, _ = bhg.plummer(n, w["seed"])
-        ms, threads = run_ref(parts, w, 2)
+        ms, threads = run_ref(gen(n), w, 2)
     return n, ms, threads
 
 
@@ -178,27 +204,49 @@ def cpu_rate(n, eval_ms, w):
     return n * w["steps"] / ((w["steps"] + 1) * t)
 
 
+def cpu_ensemble_sample(w, systems, budget_particles=600000):
+    """The reference on a seeded random subset of the ensemble's systems (one
+    evaluation each after one untimed): rate = sum N / sum eval time."""
+    order = np.random.default_rng(99).permutation(len(systems))
+    n_tot, t_tot, used, threads = 0, 0.0, 0, None
+    for s in order:
+        ms, threads = run_ref(systems[s], w, 2)
+        n_tot += len(systems[s])
+        t_tot += ms[-1] / 1000.0
+        used += 1
+        if n_tot >= budget_particles:
+            break
+    sample = (f"{used} of {len(systems)} systems ({n_tot} particles), one timed (dt, dt) evaluation each after "
+              f"one untimed, through bh::step_particles; rate = sum N / sum eval time")
+    return n_tot / t_tot, threads, sample
+
+
 def reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import bhg
 
-    n, _, _ = cpu_sample(w)
-    parts, _ = bhg.plummer(n, w["seed"])
-    ms, threads = run_ref(parts, w, args.warmup + args.steps)
-    timed = ms[args.warmup:]
-    value = cpu_rate(n, [0.0] + timed, w)
-    sample = (f"{'full system' if n == w['n'] else f'N={n} Plummer sphere (same generator and parameters)'}: "
-              f"{len(timed)} force evaluations of the reference schedule through bh::step_particles, "
-              f"rate = N*{w['steps']}/({w['steps'] + 1}*mean eval time)")
+    if w["kind"] == "ensemble":
+        systems = make_particles(w)
+        value, threads, sample = cpu_ensemble_sample(w, systems)
+        n = sum(len(p) for p in systems)
+        ms_step = n / value * 1000.0
+    else:
+        n, _, _ = cpu_sample(w)
+        parts = bhg.merger(n // 2, w["seed"]) if w["kind"] == "merger" else bhg.plummer(n, w["seed"])[0]
+        ms, threads = run_ref(parts, w, args.warmup + args.steps)
+        timed = ms[args.warmup:]
+        value = cpu_rate(n, [0.0] + timed, w)
+        ms_step = float(np.mean(timed))
+        sample = (f"{'full system' if n == w['n'] else f'N={n}, same generator and parameters'}: "
+                  f"{len(timed)} force evaluations of the reference schedule through bh::step_particles, "
+                  f"rate = N*{w['steps']}/({w['steps'] + 1}*mean eval time)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(timed)),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "n": w["n"], "sample_n": n, "theta": w["theta"], "eps": w["eps"],
-                   "max_leaf": w["max_leaf"], "target_size": w["target"], "group_size": w["group"],
-                   "dt": w["dt"], "kdk_steps": w["steps"], "threads": threads},
+        "config": {"workload": args.workload, **{k: v for k, v in w.items() if k != "kind"}, "threads": threads},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -209,172 +257,288 @@ def reference_arm(args, w):
 
 # ---------------------------------------------------------------------------- GPU arm
 
-def main():
-    args = parse()
-    w = WORKLOADS[args.workload]
-    if args.impl == "reference":
-        return reference_arm(args, w)
+class Rig:
+    """Device, stream, replicas and the timing helpers of one rank."""
 
-    import torch
+    def __init__(self):
+        import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
+        self.torch = torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
 
-        import torch.distributed as dist
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        self.stream = torch.cuda.Stream(device=self.local)
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    import bhg
+    def barrier(self):
+        self.torch.cuda.synchronize(self.local)
+        if self.world > 1:
+            self.torch.distributed.barrier()
 
-    peaks = json.load(open(MEASURED_PEAKS)) if os.path.exists(MEASURED_PEAKS) else {}
-    fp32_peak = bhg.measure_fp32_peak(local)
+    def max_over_ranks(self, v):
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([v], device=f"cuda:{self.local}")
+        self.torch.distributed.all_reduce(t, op=self.torch.distributed.ReduceOp.MAX)
+        return float(t.item())
 
-    parts, _ = bhg.plummer(w["n"], w["seed"] + rank)
+    def time_steps(self, fn, steps, warmup, after_warmup=None):
+        """Device ms of `steps` calls of fn (CUDA events on the stream) and wall
+        ms, both max over ranks, and the clock samples of the region."""
+        for _ in range(warmup):
+            fn()
+        self.barrier()
+        if after_warmup:
+            after_warmup()
+        clk = ClockSampler(self.local)
+        with clk:
+            e0 = self.torch.cuda.Event(enable_timing=True)
+            e1 = self.torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(self.stream)
+            for _ in range(steps):
+                fn()
+            e1.record(self.stream)
+            self.barrier()
+            wall = (time.perf_counter() - t0) * 1000.0
+        ms = max(e0.elapsed_time(e1), 0.0)
+        return self.max_over_ranks(ms), self.max_over_ranks(wall), clk.summary()
+
+
+def roofline(st, n_per_eval, fp32_peak, peaks):
+    flops = FLOPS_PP * st["pp"] + FLOPS_PC * st["pc"]
+    evals = max(1, st["evals"])
+    walk_ms = st["walk_ms"]
+    achieved = flops / (walk_ms / 1000.0) / 1e12 if walk_ms > 0 else 0.0
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "walk_ncu.json")
+    if os.path.exists(prof):
+        p = json.load(open(prof))
+        # the capture's DRAM bytes scale with the particles a launch processes
+        traffic = p["captured_dram_bytes"] * n_per_eval / p["captured_n"]
+    sort_bytes = n_per_eval * (8 + SORT_BYTES_PER_PASS * st["sort_passes"]) * evals
+    sort_gbs = sort_bytes / (st["sort_ms"] / 1000.0) / 1e9 if st["sort_ms"] > 0 else 0.0
+    hbm = peaks.get("hbm_gbs")
+    return {
+        "roofline": {"bound": "fp32-fma", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                     "kernel": "k_walk (force walk + fused kick/drift)",
+                     "peak_source": "measured: FFMA calibration loop on this GPU (bhg_measure_fp32_peak)",
+                     "flops_per_launch": flops / evals, "ms_per_launch": walk_ms / evals,
+                     "flop_model": "20 per particle-particle, 60 per particle-cell quadrupole interaction",
+                     "traffic_source": "profiles/walk_ncu.json: dram read+write of one captured launch, scaled "
+                                       "by particles per launch"},
+        "roofline_sort": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm, "unit": "GB/s",
+                          "frac": sort_gbs / hbm if hbm else None,
+                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy)",
+                          "bytes_model": "N*(8 + 24*passes) per sort", "ms_per_sort": st["sort_ms"] / evals},
+        "phases_ms_per_eval": {k: st[k] / evals for k in ("pre_ms", "sort_ms", "tree_ms", "multipole_ms",
+                                                          "targets_ms", "walk_ms")},
+        "interactions_per_particle": {"pp": st["pp"] / (n_per_eval * evals), "pc": st["pc"] / (n_per_eval * evals)},
+        "gpu_launches": st["kernels_per_eval"] * st["evals"],
+    }
+
+
+def force_error(ctx, parts, fp, leaf, group, target, eps2, nsample=4096):
+    """rms / p99 relative force error of one walk vs FP64 direct sum on sampled particles."""
+    ctx.upload(parts)
+    ctx.build_tree(leaf, group)
+    ctx.compute_multipoles()
+    acc = ctx.walk_forces(fp, target)  # kick = drift = 0: positions unchanged (Morton order)
+    n = len(parts)
+    idx = np.sort(np.random.default_rng(12345).choice(n, size=min(nsample, n), replace=False)).astype(np.uint32)
+    ref = ctx.direct_sum(idx, eps2)
+    rel = np.linalg.norm(acc[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    return {"vs": f"FP64 direct sum (GPU, brute_force.h semantics) on {len(idx)} sampled particles",
+            "rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99)),
+            "global": float(np.sqrt(np.sum((acc[idx] - ref) ** 2) / np.sum(ref ** 2)))}
+
+
+def cpu_single(w):
+    try:
+        ns, ems_cpu, threads = cpu_sample(w)
+        return {"value": cpu_rate(ns, ems_cpu, w), "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                "sample": (f"{'full system' if ns == w['n'] else f'N={ns}, same generator and parameters'}: "
+                           f"1 timed force evaluation (after 1 untimed) of the reference schedule through "
+                           f"bh::step_particles; rate = N*{w['steps']}/({w['steps'] + 1}*eval time)")}
+    except (OSError, subprocess.CalledProcessError) as e:
+        return {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+
+
+def bench_single(args, w, rig, bhg, fp32_peak, peaks):
+    parts = make_particles(w, rig.rank)
+    n = len(parts)
     prec = bhg.PRECISION_SPLIT if args.precision == "split" else bhg.PRECISION_FP64
     fp = bhg.Context.params(w["theta"], w["eps"] ** 2, 1.0, True, prec)
-    stream = torch.cuda.Stream(device=local)
-    ctx = bhg.Context(device=local)
-    ctx.set_stream(stream.cuda_stream)
+    ctx = bhg.Context(device=rig.local)
+    ctx.set_stream(rig.stream.cuda_stream)
     ctx.upload(parts)
 
     def one_step():
         ctx.run_schedule(fp, w["max_leaf"], w["group"], w["target"], w["dt"], w["steps"])
 
-    def barrier():
-        torch.cuda.synchronize(local)
-        if world > 1:
-            torch.distributed.barrier()
-
-    for _ in range(args.warmup):
-        one_step()
-    ctx.stats(reset=True)
-    barrier()
-    with ClockSampler(local) as clk:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            one_step()
-        e1.record(stream)
-        barrier()
-    ms = e0.elapsed_time(e1)
+    one_step()
+    ms, wall, clocks = rig.time_steps(one_step, args.steps, max(0, args.warmup - 1), lambda: ctx.stats(reset=True))
     st = ctx.stats(reset=True)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    ps = w["n"] * w["steps"] * args.steps * world
-    value = ps / (ms / 1000.0)
+    ps = n * w["steps"] * args.steps * rig.world
+    out = {"value": ps / (ms / 1000.0), "ms_per_step": ms / args.steps, "clocks": clocks,
+           **roofline(st, n, fp32_peak, peaks)}
 
-    # the walk kernel against the FP32 FMA roofline
-    flops = FLOPS_PP * st["pp"] + FLOPS_PC * st["pc"]
-    walk_ms = st["walk_ms"]
-    evals = max(1, st["evals"])
-    achieved = flops / (walk_ms / 1000.0) / 1e12 if walk_ms > 0 else 0.0
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "walk_ncu.json")
-    if os.path.exists(prof):
-        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
-    sort_bytes = w["n"] * (8 + SORT_BYTES_PER_PASS * st["sort_passes"]) * evals
-    sort_gbs = sort_bytes / (st["sort_ms"] / 1000.0) / 1e9 if st["sort_ms"] > 0 else 0.0
-    hbm = peaks.get("hbm_gbs")
-
-    # end to end through the C ABI with host buffers: H2D of the state from
-    # pinned memory, the schedule, D2H of the result, every step
-    e2e = None
     if not args.no_e2e:
-        pin = torch.empty(w["n"] * 64, dtype=torch.uint8, pin_memory=True)
+        # through the C ABI with host buffers: H2D of the state from pinned
+        # memory, the schedule, D2H of the result, every step
+        pin = rig.torch.empty(n * 64, dtype=rig.torch.uint8, pin_memory=True)
         host = np.frombuffer(pin.numpy(), dtype=bhg.PARTICLE)
         host[:] = ctx.download()
         ptr = pin.data_ptr()
 
         def e2e_step():
-            ctx._ck(ctx.L.bhg_upload(ctx.h, ptr, w["n"]))
+            ctx._ck(ctx.L.bhg_upload(ctx.h, ptr, n))
             one_step()
             ctx._ck(ctx.L.bhg_download(ctx.h, ptr))
 
-        e2e_step()
-        barrier()
-        t0 = time.perf_counter()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(args.steps):
-            e2e_step()
-        f1.record(stream)
-        barrier()
-        ems = max(f0.elapsed_time(f1), (time.perf_counter() - t0) * 1000.0)
-        if world > 1:
-            t = torch.tensor([ems], device=f"cuda:{local}")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": ps / (ems / 1000.0), "unit": "particle-steps/s", "h2d_bytes_per_step": w["n"] * 64,
-               "d2h_bytes_per_step": w["n"] * 64, "ms_per_step": ems / args.steps,
-               "path": "bhg_upload (pinned host) + bhg_run_schedule + bhg_download"}
-
-    # accuracy: rms and 99th-percentile relative force error of this walk
-    # against an FP64 direct sum on 4,096 sampled particles
-    acc_err = None
-    if rank == 0:
-        ctx.build_tree(w["max_leaf"], w["group"])
-        ctx.compute_multipoles()
-        acc = ctx.walk_forces(fp, w["target"])  # kick = drift = 0: positions unchanged
-        idx = np.sort(np.random.default_rng(12345).choice(w["n"], size=min(4096, w["n"]), replace=False))
-        ref = ctx.direct_sum(idx.astype(np.uint32), w["eps"] ** 2)
-        rel = np.linalg.norm(acc[idx] - ref, axis=1) / np.linalg.norm(ref, axis=1)
-        acc_err = {"vs": "FP64 direct sum (GPU, brute_force.h semantics) on 4096 sampled particles",
-                   "rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99)),
-                   "global": float(np.sqrt(np.sum((acc[idx] - ref) ** 2) / np.sum(ref ** 2)))}
-
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        try:
-            n, ems_cpu, threads = cpu_sample(w)
-            cpu = {"value": cpu_rate(n, ems_cpu, w), "unit": "particle-steps/s", "cores": threads,
-                   "kind": "reference",
-                   "sample": (f"{'full system' if n == w['n'] else f'N={n} Plummer sphere, same parameters'}: "
-                              f"1 timed force evaluation (after 1 untimed) of the reference schedule through "
-                              f"bh::step_particles; rate = N*{w['steps']}/({w['steps'] + 1}*eval time)")}
-        except (OSError, subprocess.CalledProcessError) as e:
-            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
-                   "sample": f"unavailable: {e}"}
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64" if prec == bhg.PRECISION_SPLIT else "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "n": w["n"], "seed": w["seed"], "theta": w["theta"],
-                       "eps": w["eps"], "max_leaf": w["max_leaf"], "target_size": w["target"],
-                       "group_size": w["group"], "dt": w["dt"], "kdk_steps_per_bench_step": w["steps"],
-                       "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (particles 256 MB + tree ~150 MB per evaluation)"},
-            "gpu_launches": st["kernels_per_eval"] * st["evals"],
-            "roofline": {"bound": "fp32-fma", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
-                         "kernel": "k_walk (force walk + fused kick/drift)",
-                         "peak_source": "measured: FFMA calibration loop on this GPU (bhg_measure_fp32_peak)",
-                         "flops_per_launch": flops / evals, "ms_per_launch": walk_ms / evals,
-                         "flop_model": "20 per particle-particle, 60 per particle-cell quadrupole interaction"},
-            "roofline_sort": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm, "unit": "GB/s",
-                              "frac": sort_gbs / hbm if hbm else None,
-                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy)",
-                              "bytes_model": "N*(8 + 24*passes) per sort", "ms_per_sort": st["sort_ms"] / evals},
-            "phases_ms_per_eval": {k: st[k] / evals for k in ("pre_ms", "sort_ms", "tree_ms", "multipole_ms",
-                                                              "targets_ms", "walk_ms")},
-            "interactions_per_particle": {"pp": st["pp"] / (w["n"] * evals), "pc": st["pc"] / (w["n"] * evals)},
-            "clocks": clk.summary(),
-            "force_error": acc_err,
-            "e2e": e2e,
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
+        ems, ewall, _ = rig.time_steps(e2e_step, args.steps, 1)
+        ems = max(ems, ewall)
+        out["e2e"] = {"value": ps / (ems / 1000.0), "unit": "particle-steps/s", "h2d_bytes_per_step": n * 64,
+                      "d2h_bytes_per_step": n * 64, "ms_per_step": ems / args.steps,
+                      "path": "bhg_upload (pinned host) + bhg_run_schedule + bhg_download"}
+    if rig.rank == 0:
+        out["force_error"] = force_error(ctx, parts, fp, w["max_leaf"], w["group"], w["target"], w["eps"] ** 2)
     ctx.close()
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    if rig.rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_single(w)
+    out["config_extra"] = {"n": n}
+    return out
+
+
+def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
+    from bhg import autotune
+
+    systems = make_particles(w, rig.rank)
+    ns = len(systems)
+    n = sum(len(p) for p in systems)
+    eps2 = w["eps"] ** 2
+    tuned = autotune.tune(systems, w["theta"], eps2, w["group"], bhg.PRECISION_SPLIT, device=rig.local)
+    leaf = tuned["max_leaf"]
+    fp = bhg.Context.params(w["theta"], eps2, 1.0, True, bhg.PRECISION_SPLIT)
+    ctx = bhg.Context(device=rig.local)
+    ctx.set_stream(rig.stream.cuda_stream)
+    ctx.upload_systems(systems)
+    ones = np.ones(ns)
+
+    def one_step():  # one lockstep KDK evaluation of every system
+        ctx.set_system_params(theta=ones * w["theta"], eps2=ones * eps2, kick_dt=ones * w["dt"],
+                              drift_dt=ones * w["dt"])
+        ctx.step_systems(fp, leaf, w["group"], leaf)
+
+    one_step()
+    ms, wall, clocks = rig.time_steps(one_step, args.steps, max(0, args.warmup - 1), lambda: ctx.stats(reset=True))
+    st = ctx.stats(reset=True)
+    ps = n * args.steps * rig.world
+    out = {"value": ps / (ms / 1000.0), "ms_per_step": ms / args.steps, "clocks": clocks,
+           **roofline(st, n, fp32_peak, peaks),
+           "autotune": {k: tuned[k] for k in ("max_leaf", "target_size", "rms_error", "err_budget", "table")}}
+
+    if not args.no_e2e:
+        flat = np.concatenate(systems)
+        pin = rig.torch.empty(n * 64, dtype=rig.torch.uint8, pin_memory=True)
+        host = np.frombuffer(pin.numpy(), dtype=bhg.PARTICLE)
+        host[:] = flat
+        ptr = pin.data_ptr()
+        counts = np.array([len(p) for p in systems], np.uint64)
+
+        def e2e_step():
+            ctx._ck(ctx.L.bhg_upload_systems(ctx.h, ptr, counts.ctypes.data, ns))
+            one_step()
+            ctx._ck(ctx.L.bhg_download(ctx.h, ptr))
+
+        ems, ewall, _ = rig.time_steps(e2e_step, args.steps, 1)
+        ems = max(ems, ewall)
+        out["e2e"] = {"value": ps / (ems / 1000.0), "unit": "particle-steps/s", "h2d_bytes_per_step": n * 64,
+                      "d2h_bytes_per_step": n * 64, "ms_per_step": ems / args.steps,
+                      "path": "bhg_upload_systems (pinned host) + bhg_step_systems + bhg_download"}
+    if rig.rank == 0:
+        big = systems[int(np.argmax([len(p) for p in systems]))]
+        out["force_error"] = force_error(ctx, big, fp, leaf, w["group"], leaf, eps2)
+        out["force_error"]["system"] = f"largest system (N={len(big)}) at the tuned leaf {leaf}"
+    ctx.close()
+
+    if not args.no_plain:
+        # the plain FP64 path, one system at a time: a resident context per
+        # system, each evaluation stepping the 512 contexts in turn with the
+        # reference's leaf/target/group sizes
+        fp64 = bhg.Context.params(w["theta"], eps2, 1.0, True, bhg.PRECISION_FP64)
+        ctxs = []
+        for p in systems:
+            c = bhg.Context(device=rig.local)
+            c.upload(p)
+            ctxs.append(c)
+
+        def plain_step():
+            for c in ctxs:
+                c.step(fp64, w["max_leaf"], w["group"], w["target"], w["dt"], w["dt"])
+
+        plain_step()
+        rig.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            plain_step()
+        rig.barrier()
+        pms = rig.max_over_ranks((time.perf_counter() - t0) * 1000.0)
+        for c in ctxs:
+            c.close()
+        pv = ps / (pms / 1000.0)
+        out["plain_fp64_one_at_a_time"] = {
+            "value": pv, "unit": "particle-steps/s", "ms_per_step": pms / args.steps,
+            "path": "512 resident contexts stepped in turn, FP64 walk, leaf/target 16, group 256 (wall clock)"}
+        out["speedup_vs_plain"] = out["value"] / pv
+
+    if rig.rank == 0 and not args.no_cpu_baseline:
+        try:
+            v, threads, sample = cpu_ensemble_sample(w, systems)
+            out["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                                   "sample": sample}
+        except (OSError, subprocess.CalledProcessError) as e:
+            out["cpu_baseline"] = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    out["config_extra"] = {"systems": ns, "n_total": n, "max_leaf_tuned": leaf}
+    return out
+
+
+def main():
+    args = parse()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return reference_arm(args, w)
+    rig = Rig()
+    import bhg
+
+    peaks = json.load(open(MEASURED_PEAKS)) if os.path.exists(MEASURED_PEAKS) else {}
+    fp32_peak = bhg.measure_fp32_peak(rig.local)
+    if w["kind"] == "ensemble":
+        res = bench_ensemble(args, w, rig, bhg, fp32_peak, peaks)
+        dtype = "f32+f64"
+    else:
+        res = bench_single(args, w, rig, bhg, fp32_peak, peaks)
+        dtype = "f32+f64" if args.precision == "split" else "f64"
+    if rig.rank == 0:
+        cfg = {"workload": args.workload, **{k: v for k, v in w.items() if k != "kind"},
+               **res.pop("config_extra"), "precision": args.precision if w["kind"] != "ensemble" else "split",
+               "parallelism": f"replicas x{rig.world}",
+               "l2": "inputs larger than L2 (particle state, Morton copy and tree exceed 126 MB)"}
+        line = {"metric": METRIC, "value": res.pop("value"), "unit": "particle-steps/s", "n_gpus": rig.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+                "data": "synthetic", "config": cfg, **res}
+        print(json.dumps(line), flush=True)
+    if rig.world > 1:
+        rig.torch.distributed.barrier()
+        rig.torch.distributed.destroy_process_group()
     return 0
 
 

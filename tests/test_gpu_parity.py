@@ -200,3 +200,25 @@ def test_hbm_budget_is_enforced():
         ctx.upload(cube(100000, 1))
     assert e.value.code == bhg.ENOMEM
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
+def test_system_alone_equals_in_the_mix(precision):
+    # a system's step does not depend on the systems batched beside it: bit
+    # for bit the same particles alone and inside a 5-system batch
+    systems = [bhg.plummer(n, 200 + i)[0] for i, n in enumerate((3000, 12000, 1100, 40000, 7000))]
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, precision)
+    with bhg.Context(device=0) as mix:
+        mix.upload_systems(systems)
+        mix.set_system_params(theta=np.full(5, 0.5), eps2=np.full(5, 1e-4), kick_dt=np.full(5, 0.01),
+                              drift_dt=np.full(5, 0.01))
+        mix.step_systems(fp, 16, 256, 16)
+        out = mix.download()
+    at = 0
+    with bhg.Context(device=0) as alone:
+        for s in systems:
+            alone.upload(s)
+            alone.step(fp, 16, 256, 16, 0.01, 0.01)
+            got = alone.download()
+            assert got.tobytes() == out[at:at + len(s)].tobytes()
+            at += len(s)
