@@ -30,7 +30,8 @@ EXPORT_KEYS, EXPORT_PERM, EXPORT_NODES_U32, EXPORT_NODES_F64, EXPORT_DOMAINS, EX
 #: Every entry point include/bhg.h declares.
 EXPORTED = (
     "bhg_create", "bhg_destroy", "bhg_last_error", "bhg_set_stream", "bhg_upload", "bhg_upload_device",
-    "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_build_tree",
+    "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_add_system",
+    "bhg_add_generated", "bhg_remove_systems", "bhg_num_systems", "bhg_system_ids", "bhg_build_tree",
     "bhg_compute_multipoles", "bhg_walk_forces", "bhg_integrate", "bhg_step", "bhg_step_systems",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
     "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
@@ -42,6 +43,11 @@ class BhgError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"bhg error {code}: {msg}")
         self.code = code
+
+
+class Sphere(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("a", C.c_double), ("mass", C.c_double), ("centre", C.c_double * 3),
+                ("bulk", C.c_double * 3)]
 
 
 class Config(C.Structure):
@@ -89,6 +95,11 @@ def lib() -> C.CDLL:
         "bhg_download": ([vp, vp], i32),
         "bhg_download_device": ([vp, vp], i32),
         "bhg_num_particles": ([vp], sz),
+        "bhg_add_system": ([vp, vp, sz, C.POINTER(u64)], i32),
+        "bhg_add_generated": ([vp, vp, i32, u64, u32, C.POINTER(u64)], i32),
+        "bhg_remove_systems": ([vp, vp, sz, vp], i32),
+        "bhg_num_systems": ([vp], sz),
+        "bhg_system_ids": ([vp, vp], i32),
         "bhg_build_tree": ([vp, C.c_uint, u32], i32),
         "bhg_compute_multipoles": ([vp], i32),
         "bhg_walk_forces": ([vp, C.POINTER(ForceParams), u32, f64, f64, vp, vp], i32),
@@ -201,6 +212,46 @@ class Context:
         counts = np.array([len(s) for s in systems], np.uint64)
         self._ck(self.L.bhg_upload_systems(self.h, _p(parts), _p(counts), len(counts)))
         self.n = len(parts)
+
+    def add_system(self, parts) -> int:
+        """Appends one system (host particles); returns its handle."""
+        parts = np.ascontiguousarray(parts, PARTICLE)
+        h = C.c_uint64()
+        self._ck(self.L.bhg_add_system(self.h, _p(parts), len(parts), C.byref(h)))
+        self.n = self.L.bhg_num_particles(self.h)
+        return h.value
+
+    def add_generated(self, spheres, seed, id0=0) -> int:
+        """Appends one system generated on the device from `seed`: one or two
+        spheres, each a dict with n, a, mass and optional centre, bulk."""
+        arr = (Sphere * len(spheres))()
+        for k, sp in enumerate(spheres):
+            arr[k] = Sphere(int(sp["n"]), float(sp.get("a", 1.0)), float(sp.get("mass", 1.0)),
+                            (C.c_double * 3)(*sp.get("centre", (0.0, 0.0, 0.0))),
+                            (C.c_double * 3)(*sp.get("bulk", (0.0, 0.0, 0.0))))
+        h = C.c_uint64()
+        self._ck(self.L.bhg_add_generated(self.h, arr, len(spheres), int(seed) % (1 << 64), id0, C.byref(h)))
+        self.n = self.L.bhg_num_particles(self.h)
+        return h.value
+
+    def remove_systems(self, handles, want=False, sizes=None):
+        """Removes systems by handle.  want: also return their particles, a
+        list of arrays (sizes: their particle counts, in the same order)."""
+        hs = np.ascontiguousarray(handles, np.uint64)
+        out = None
+        if want:
+            out = np.zeros(int(sum(sizes)), PARTICLE)
+        self._ck(self.L.bhg_remove_systems(self.h, _p(hs), len(hs), None if out is None else _p(out)))
+        self.n = self.L.bhg_num_particles(self.h)
+        if out is None:
+            return None
+        return np.split(out, np.cumsum(sizes)[:-1])
+
+    def system_ids(self) -> np.ndarray:
+        out = np.zeros(self.L.bhg_num_systems(self.h), np.uint64)
+        if len(out):
+            self._ck(self.L.bhg_system_ids(self.h, _p(out)))
+        return out
 
     def download(self) -> np.ndarray:
         out = np.zeros(self.n, PARTICLE)

@@ -30,16 +30,20 @@ struct bhg_context {
   uint64_t budget = 0, allocated = 0;
   std::string err;
 
-  // current problem
+  // current problem: systems back to back, each with a handle
   size_t n = 0;
   int nsys = 0;
+  std::vector<uint64_t> counts, ids;
+  uint64_t next_id = 1;
   std::vector<SysDev> sys_host;
   std::vector<SysParam> prm_host;
   std::vector<Tile> tiles_host;
   std::vector<std::pair<void*, size_t>> allocs;
 
   // capacities
-  size_t cap_n = 0, cap_nodes = 0, cap_sys = 0, cap_tiles = 0, cap_stack_warps = 0;
+  // capacities (cap_n covers the scratch, cap_part the state; a capacity is
+  // 0 after a growth that failed part-way)
+  size_t cap_n = 0, cap_part = 0, cap_nodes = 0, cap_sys = 0, cap_tiles = 0, cap_stack_warps = 0;
 
   // device buffers
   Particle *part = nullptr, *staged = nullptr;
@@ -138,6 +142,14 @@ void drop_graph(bhg_context* c) {
   }
 }
 
+// Device bytes of one node slot (the SoA arrays, the walk record, the cut
+// lists) and of the slots one particle brings at max_leaf 16 (0.45 each).
+constexpr size_t kNodeBytes = 16 + 32 + 32 + 48 + 64 + 8 + 48 + 12 + 4;
+constexpr size_t kNodeBytesPerParticle = kNodeBytes * 45 / 100;
+// Device bytes of the particle-sized buffers, per particle: the state and
+// its staging copy, sources, sort keys and values, marks, accelerations.
+constexpr size_t kParticleBytes = 2 * sizeof(Particle) + sizeof(double4) + 24 + 4 + 24;
+
 // Node slots for n particles: about 0.25 per particle at max_leaf 16 on
 // Plummer spheres, up to ~1.5 at max_leaf 1; grown on overflow.
 size_t node_estimate(size_t n, int nsys, unsigned max_leaf) {
@@ -148,7 +160,13 @@ size_t node_estimate(size_t n, int nsys, unsigned max_leaf) {
 int ensure_nodes(bhg_context* c, size_t need) {
   if (need <= c->cap_nodes) return BHG_OK;
   size_t cap = need;
+  if (c->cap_nodes > 0) {  // systems come and go: grow with slack, within the budget
+    const size_t want = std::max(need, c->cap_nodes + c->cap_nodes / 2);
+    if (!c->budget || c->allocated + (want - c->cap_nodes) * kNodeBytes <= c->budget) cap = want;
+  }
   drop_graph(c);
+  c->cap_nodes = 0;  // until every array below exists again
+  c->nd.cap = 0;
   int r;
   if ((r = grow(c, &c->nd.begin, cap)) || (r = grow(c, &c->nd.count, cap)) || (r = grow(c, &c->nd.first, cap)) ||
       (r = grow(c, &c->nd.info, cap)) || (r = grow(c, &c->nd.box, cap)) || (r = grow(c, &c->nd.mom, cap)) ||
@@ -162,14 +180,43 @@ int ensure_nodes(bhg_context* c, size_t need) {
   return BHG_OK;
 }
 
-// Particle-sized buffers and the per-system tables for the current problem.
+// Particle-sized buffers and the per-system tables for n particles.  The
+// state (c->part) keeps its first c->n particles across a growth, so
+// systems can be added to a resident set.  A growth that fails part-way
+// leaves the state intact and the failed capacity at 0: the next call
+// allocates that group of buffers again.
 int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles) {
   int r;
+  if (n > c->cap_n && c->cap_n > 0) {
+    // systems are added one at a time: grow with slack, within the budget
+    // (counting the node slots the extra particles bring too)
+    const size_t want = std::max(n, c->cap_n + c->cap_n / 2);
+    if (!c->budget || c->allocated + (want - c->cap_n) * (kParticleBytes + kNodeBytesPerParticle) <= c->budget)
+      n = want;
+  }
   if (n > c->cap_n) {
+    // the scratch goes first, so that the state's old and new copies are
+    // the only large buffers alive at once
     drop_graph(c);
-    dev_free(c, c->accel);
-    c->accel = nullptr;
-    if ((r = grow(c, &c->part, n)) || (r = grow(c, &c->staged, n)) || (r = grow(c, &c->pm, n)) ||
+    c->cap_n = 0;
+    dev_free(c, c->accel), dev_free(c, c->staged), dev_free(c, c->pm), dev_free(c, c->mark), dev_free(c, c->scan_lb);
+    c->accel = nullptr, c->staged = nullptr, c->pm = nullptr, c->mark = nullptr, c->scan_lb = nullptr;
+    for (int k = 0; k < 2; ++k) {
+      dev_free(c, c->keys[k]), dev_free(c, c->vals[k]);
+      c->keys[k] = nullptr, c->vals[k] = nullptr;
+    }
+    if (n > c->cap_part) {
+      Particle* np = nullptr;
+      if ((r = dev_alloc(c, reinterpret_cast<void**>(&np), n * sizeof(Particle)))) return r;
+      if (c->part && c->n) CK(cudaMemcpyAsync(np, c->part, c->n * sizeof(Particle), cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      dev_free(c, c->part);
+      c->part = np;
+      c->cap_part = n;
+    }
+    // the staging buffer trades places with the state (bhg_remove_systems):
+    // both have the state's capacity
+    if ((r = grow(c, &c->staged, c->cap_part)) || (r = grow(c, &c->pm, n)) ||
         (r = grow(c, &c->keys[0], n)) || (r = grow(c, &c->keys[1], n)) || (r = grow(c, &c->vals[0], n)) ||
         (r = grow(c, &c->vals[1], n)) || (r = grow(c, &c->mark, n)) || (r = grow(c, &c->scan_lb, 2 * (n / 4096) + 32)))
       return r;
@@ -177,14 +224,18 @@ int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles) {
     c->cap_n = n;
   }
   if ((size_t)nsys > c->cap_sys) {
+    nsys = (int)std::max<size_t>((size_t)nsys, c->cap_sys + c->cap_sys / 2);
     drop_graph(c);
+    c->cap_sys = 0;
     if ((r = grow(c, &c->sys, nsys)) || (r = grow(c, &c->prm, nsys)) ||
         (r = grow(c, &c->hist, (size_t)nsys * kSortPasses * 256)) || (r = grow(c, &c->offs, (size_t)nsys * kSortPasses * 256)))
       return r;
     c->cap_sys = nsys;
   }
   if (ntiles > c->cap_tiles) {
+    ntiles = std::max(ntiles, c->cap_tiles + c->cap_tiles / 2);
     drop_graph(c);
+    c->cap_tiles = 0;
     if ((r = grow(c, &c->tiles, ntiles)) || (r = grow(c, &c->partial, ntiles * 6)) ||
         (r = grow(c, &c->sort_lb, ntiles * kSortPasses * 256)))
       return r;
@@ -206,18 +257,21 @@ int ensure_stack(bhg_context* c, int grid) {
   return BHG_OK;
 }
 
-// Lays out systems and sort tiles for particle counts `counts`.
-int set_problem(bhg_context* c, const uint64_t* counts, size_t nsys) {
-  if (nsys == 0) return fail(c, BHG_EINVAL, "no systems");
+// Lays out the systems c->counts back to back with their sort tiles, sizes
+// the buffers for them (the state's first c->n particles survive a growth)
+// and resets the per-step device state.  Per-system parameters stay with
+// their systems; new systems get the defaults.
+int relayout(bhg_context* c) {
+  const size_t nsys = c->counts.size();
   size_t n = 0, ntiles = 0;
   for (size_t s = 0; s < nsys; ++s) {
-    if (counts[s] == 0) return fail(c, BHG_EINVAL, "system " + std::to_string(s) + " has no particles");
-    n += counts[s];
-    ntiles += (counts[s] + kTile - 1) / kTile;
+    if (c->counts[s] == 0) return fail(c, BHG_EINVAL, "system " + std::to_string(s) + " has no particles");
+    n += c->counts[s];
+    ntiles += (c->counts[s] + kTile - 1) / kTile;
   }
   if (n >= (1ull << 30)) return fail(c, BHG_EINVAL, "more than 2^30 - 1 particles");
   if (nsys > 65535) return fail(c, BHG_EINVAL, "more than 65535 systems");
-  int r = ensure_particles(c, n, (int)nsys, ntiles);
+  int r = ensure_particles(c, n, (int)std::max<size_t>(nsys, 1), std::max<size_t>(ntiles, 1));
   if (r) return r;
   c->sys_host.assign(nsys, SysDev{});
   c->tiles_host.clear();
@@ -225,7 +279,7 @@ int set_problem(bhg_context* c, const uint64_t* counts, size_t nsys) {
   for (size_t s = 0; s < nsys; ++s) {
     SysDev& d = c->sys_host[s];
     d.begin = begin;
-    d.n = (uint32_t)counts[s];
+    d.n = (uint32_t)c->counts[s];
     d.root = (uint32_t)s;
     d.tile_begin = (uint32_t)c->tiles_host.size();
     for (uint32_t o = 0; o < d.n; o += kTile)
@@ -236,13 +290,38 @@ int set_problem(bhg_context* c, const uint64_t* counts, size_t nsys) {
   if (c->n != n || c->nsys != (int)nsys) drop_graph(c);
   c->n = n;
   c->nsys = (int)nsys;
-  c->prm_host.assign(nsys, SysParam{0.25, 0.0, 1.0, 0.0, 0.0, {0, 0, 0}});
-  CK(cudaMemcpyAsync(c->sys, c->sys_host.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->tiles, c->tiles_host.data(), c->tiles_host.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+  c->prm_host.resize(nsys, SysParam{0.25, 0.0, 1.0, 0.0, 0.0, {0, 0, 0}});
+  if (nsys) {
+    CK(cudaMemcpyAsync(c->sys, c->sys_host.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->tiles, c->tiles_host.data(), c->tiles_host.size() * sizeof(Tile), cudaMemcpyHostToDevice,
+                       c->stream));
+  }
+  // a new layout starts with clear error bits and per-build/per-walk fields;
+  // the interaction totals and the evaluation count run on until reset
+  CK(cudaMemsetAsync(&c->st->status, 0, sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(reinterpret_cast<char*>(c->st) + kBuildResetOffset, 0, sizeof(DevState) - kBuildResetOffset,
                      c->stream));
-  CK(cudaMemsetAsync(c->st, 0, sizeof(DevState), c->stream));
   c->built = c->moments = c->walked = false;
   return BHG_OK;
+}
+
+// A fresh set of systems (bhg_upload*): new handles, default parameters,
+// nothing of the old state carried over.
+int set_problem(bhg_context* c, const uint64_t* counts, size_t nsys) {
+  if (nsys == 0) return fail(c, BHG_EINVAL, "no systems");
+  c->counts.assign(counts, counts + nsys);
+  c->ids.resize(nsys);
+  for (size_t s = 0; s < nsys; ++s) c->ids[s] = c->next_id++;
+  c->prm_host.clear();
+  c->n = 0;
+  return relayout(c);
+}
+
+// After a growth that failed part-way some scratch may be missing (its
+// capacity is then 0): allocates it again before anything is launched.
+int ensure_layout(bhg_context* c) {
+  if (c->cap_n >= c->n && c->cap_sys >= c->counts.size() && c->cap_tiles >= c->tiles_host.size()) return BHG_OK;
+  return relayout(c);
 }
 
 // ---- enqueue the phases (no host synchronisation) ---------------------------
@@ -567,15 +646,141 @@ int bhg_download_device(bhg_context* c, void* out) {
 
 size_t bhg_num_particles(const bhg_context* c) { return c ? c->n : 0; }
 
+}  // extern "C"
+
+// Appends one system of n particles, written into the state by fill(dst);
+// on failure the resident systems are untouched.
+template <typename F>
+static int add_system_impl(bhg_context* c, size_t n, uint64_t* id, F fill) {
+  if (!c) return BHG_EINVAL;
+  if (n == 0) return fail(c, BHG_EINVAL, "empty system");
+  cudaSetDevice(c->device);
+  const size_t old = c->n;
+  c->counts.push_back(n);
+  c->ids.push_back(c->next_id);
+  int r = relayout(c);
+  if (r) {
+    const std::string why = c->err;
+    c->counts.pop_back();
+    c->ids.pop_back();
+    c->n = old;
+    relayout(c);  // a failure here leaves capacities at 0, which the next call repairs
+    return fail(c, r, why);
+  }
+  if ((r = fill(c->part + old))) return r;
+  if (id) *id = c->next_id;
+  ++c->next_id;
+  return BHG_OK;
+}
+
+extern "C" {
+
+int bhg_add_system(bhg_context* c, const bh_particle64* p, size_t n, uint64_t* id) {
+  if (!c) return BHG_EINVAL;
+  if (!p) return fail(c, BHG_EINVAL, "null particles");
+  return add_system_impl(c, n, id, [&](Particle* dst) -> int {
+    CK(cudaMemcpyAsync(dst, p, n * sizeof(Particle), cudaMemcpyHostToDevice, c->stream));
+    return BHG_OK;
+  });
+}
+
+int bhg_add_generated(bhg_context* c, const bhg_sphere* spheres, int nspheres, uint64_t seed, uint32_t id0,
+                      uint64_t* id) {
+  if (!c) return BHG_EINVAL;
+  if (!spheres || nspheres < 1 || nspheres > 2) return fail(c, BHG_EINVAL, "one or two spheres");
+  size_t n = 0;
+  for (int k = 0; k < nspheres; ++k) {
+    if (spheres[k].n == 0 || !(spheres[k].a > 0.0) || !(spheres[k].mass > 0.0))
+      return fail(c, BHG_EINVAL, "a sphere needs n > 0, a > 0 and mass > 0");
+    n += spheres[k].n;
+  }
+  return add_system_impl(c, n, id, [&](Particle* dst) -> int {
+    size_t at = 0;
+    for (int k = 0; k < nspheres; ++k) {
+      const bhg_sphere& sp = spheres[k];
+      // the second sphere draws from its own stream of the same seed
+      launch_plummer(dst + at, (uint32_t)sp.n, sp.a, sp.mass, sp.centre, sp.bulk, id0 + (uint32_t)at,
+                     seed + 0x9E3779B97F4A7C15ull * (uint64_t)k, c->sms, c->stream);
+      at += sp.n;
+    }
+    CK(cudaGetLastError());
+    return BHG_OK;
+  });
+}
+
+int bhg_remove_systems(bhg_context* c, const uint64_t* handles, size_t k, bh_particle64* out) {
+  if (!c) return BHG_EINVAL;
+  if (!handles && k) return fail(c, BHG_EINVAL, "null handles");
+  cudaSetDevice(c->device);
+  std::vector<size_t> pos(k);
+  std::vector<uint64_t> start(c->counts.size() + 1, 0);
+  for (size_t s = 0; s < c->counts.size(); ++s) start[s + 1] = start[s] + c->counts[s];
+  std::vector<char> gone(c->counts.size(), 0);
+  for (size_t i = 0; i < k; ++i) {
+    auto it = std::find(c->ids.begin(), c->ids.end(), handles[i]);
+    if (it == c->ids.end()) return fail(c, BHG_EINVAL, "no system with handle " + std::to_string(handles[i]));
+    pos[i] = (size_t)(it - c->ids.begin());
+    if (gone[pos[i]]) return fail(c, BHG_EINVAL, "handle given twice");
+    gone[pos[i]] = 1;
+  }
+  // the packing goes through the staging buffer, which a growth that failed
+  // part-way may have left unallocated
+  if (!c->staged && c->cap_part) {
+    int r = dev_alloc(c, reinterpret_cast<void**>(&c->staged), c->cap_part * sizeof(Particle));
+    if (r) return r;
+  }
+  if (out) {  // the removed systems' particles, back to back in the given order
+    size_t at = 0;
+    for (size_t i = 0; i < k; ++i) {
+      const size_t s = pos[i];
+      CK(cudaMemcpyAsync(out + at, c->part + start[s], c->counts[s] * sizeof(Particle), cudaMemcpyDeviceToHost,
+                         c->stream));
+      at += c->counts[s];
+    }
+  }
+  // the kept systems, packed into the staging buffer, which becomes the state
+  size_t at = 0;
+  std::vector<uint64_t> counts, ids;
+  std::vector<SysParam> prm;
+  for (size_t s = 0; s < c->counts.size(); ++s) {
+    if (gone[s]) continue;
+    CK(cudaMemcpyAsync(c->staged + at, c->part + start[s], c->counts[s] * sizeof(Particle), cudaMemcpyDeviceToDevice,
+                       c->stream));
+    at += c->counts[s];
+    counts.push_back(c->counts[s]);
+    ids.push_back(c->ids[s]);
+    prm.push_back(c->prm_host[s]);
+  }
+  std::swap(c->part, c->staged);
+  c->counts = counts;
+  c->ids = ids;
+  c->prm_host = prm;
+  c->n = at;
+  drop_graph(c);  // the state moved to the other buffer
+  int r = relayout(c);
+  if (r) return r;
+  if (out) CK(cudaStreamSynchronize(c->stream));
+  return BHG_OK;
+}
+
+size_t bhg_num_systems(const bhg_context* c) { return c ? c->counts.size() : 0; }
+
+int bhg_system_ids(const bhg_context* c, uint64_t* out) {
+  if (!c || !out) return BHG_EINVAL;
+  std::copy(c->ids.begin(), c->ids.end(), out);
+  return BHG_OK;
+}
+
 int bhg_build_tree(bhg_context* c, unsigned max_leaf, uint32_t group_size) {
   if (!c) return BHG_EINVAL;
   if (c->n == 0) return fail(c, BHG_ESTATE, "no particles uploaded");
   if (max_leaf == 0) return fail(c, BHG_EINVAL, "max_leaf must be >= 1");
   cudaSetDevice(c->device);
+  int r = ensure_layout(c);
+  if (r) return r;
   c->max_leaf = max_leaf;
   c->group_size = group_size;
-  int r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf));
-  if (r) return r;
+  if ((r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf)))) return r;
   for (int attempt = 0; attempt < 8; ++attempt) {
     if ((r = run_build(c, false, ""))) return r;
     if ((r = read_state(c))) return r;
@@ -683,7 +888,7 @@ int prepare_step(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, 
   if (max_leaf == 0) return fail(c, BHG_EINVAL, "max_leaf must be >= 1");
   cudaSetDevice(c->device);
   int r = set_force_params(c, fp, kick, drift, keep);
-  if (r) return r;
+  if (r || (r = ensure_layout(c))) return r;
   if (c->max_leaf != max_leaf || c->group_size != group_size) drop_graph(c);
   c->max_leaf = max_leaf;
   c->group_size = group_size;

@@ -67,5 +67,10 @@ void launch_direct(const double4* pm, uint32_t begin, uint32_t n, const uint32_t
                    double G, double* out, cudaStream_t s);
 void launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int sms, cudaStream_t s);
 double measure_fp32_peak(int device);
+// n particles of one Plummer sphere (scale a, total mass `mass`, centre c[3],
+// bulk velocity b[3], ids id0..), drawn from a counter-based generator keyed
+// by `seed`.
+void launch_plummer(Particle* out, uint32_t n, double a, double mass, const double* c, const double* b, uint32_t id0,
+                    uint64_t seed, int sms, cudaStream_t s);
 
 }  // namespace bhg

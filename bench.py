@@ -19,6 +19,14 @@ Other workloads (--workload):
                 segmented key space, split precision, leaf/target sizes from
                 the autotuner; also times the plain FP64 path looping over
                 the systems one at a time (the north-star comparison)
+  serve-200rps  configs[4]: Poisson arrivals at 200 requests/s for 60 s, each
+                a Plummer sphere or a merger (50/50), N log-uniform in
+                [4,096, 2,097,152], 16-256 steps, theta from {0.4, 0.5, 0.7},
+                eps 0.01, dt 1/128, generated on the device from a
+                per-request seed and served by continuous batching under a
+                150 GB HBM admission budget; reports p50/p99 per-step latency
+                and aggregate particle-steps/s over a bounded wall window
+                (120 s; --steps/--warmup do not apply)
   plummer-1m    a smaller case of configs[1] for profiler captures
 
 --impl reference times the reference's own CPU implementation of the path
@@ -54,6 +62,9 @@ WORKLOADS = {
                        group=256, dt=1.0 / 256, steps=8),
     "ensemble-512": dict(kind="ensemble", nsys=512, seed=3, theta=0.5, eps=0.01, max_leaf=16, target=16, group=256,
                          dt=1.0 / 128, steps=32),
+    "serve-200rps": dict(kind="serve", rate=200.0, duration=60.0, seed=5, nmin=4096, nmax=2097152, smin=16,
+                         smax=256, thetas=(0.4, 0.5, 0.7), eps=0.01, dt=1.0 / 128, max_leaf=16, target=16,
+                         group=256, hbm_budget_gb=150.0, wall_limit_s=120.0),
 }
 METRIC = "particle-steps/s"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -72,6 +83,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="ensemble: skip the one-at-a-time FP64 path")
+    ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
+    ap.add_argument("--serve-wall", type=float, default=None, help="serve: wall-clock window in seconds")
+    ap.add_argument("--serve-duration", type=float, default=None, help="serve: length of the arrival stream")
     return ap.parse_args()
 
 
@@ -221,13 +235,57 @@ def cpu_ensemble_sample(w, systems, budget_particles=600000):
     return n_tot / t_tot, threads, sample
 
 
+def serve_request_particles(req):
+    """A served request's initial conditions drawn by the host generator (the
+    distribution of the device generator)."""
+    import bhg
+
+    seed = req.seed % (1 << 63)
+    if req.kind == "plummer":
+        return bhg.plummer(req.n, seed)[0]
+    sp = req.spheres()
+    p1, nxt = bhg.plummer(sp[0]["n"], seed, a=sp[0]["a"], centre=sp[0]["centre"], bulk=sp[0]["bulk"])
+    p2, _ = bhg.plummer(sp[1]["n"], nxt, a=sp[1]["a"], centre=sp[1]["centre"], bulk=sp[1]["bulk"], id0=sp[0]["n"])
+    return np.concatenate([p1, p2])
+
+
+def serve_stream(w):
+    from bhg import serve
+
+    return serve.poisson_stream(w["rate"], w["duration"], w["seed"], w["nmin"], w["nmax"], w["smin"], w["smax"],
+                                w["thetas"])
+
+
+def cpu_serve_sample(w, budget_particles=600000):
+    """The reference on the stream's first requests, one at a time (it serves
+    one simulation per process): one timed (dt, dt) evaluation per request
+    after one untimed, at the request's own theta.  Returns (rate, threads, sample)."""
+    n_tot, t_tot, used, threads = 0, 0.0, 0, None
+    for r in serve_stream(w):
+        if n_tot + r.n > budget_particles:
+            continue
+        ms, threads = run_ref(serve_request_particles(r), dict(w, theta=r.theta, steps=r.steps), 2)
+        n_tot += r.n
+        t_tot += ms[-1] / 1000.0
+        used += 1
+        if n_tot >= budget_particles * 0.9:
+            break
+    sample = (f"the stream's first {used} requests that fit {budget_particles} particles ({n_tot} particles), "
+              f"one at a time through bh::step_particles, one timed (dt, dt) evaluation each after one untimed; "
+              f"rate = sum N / sum eval time")
+    return n_tot / t_tot, threads, sample
+
+
 def reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import bhg
 
-    if w["kind"] == "ensemble":
+    if w["kind"] == "serve":
+        value, threads, sample = cpu_serve_sample(w)
+        ms_step = None
+    elif w["kind"] == "ensemble":
         systems = make_particles(w)
         value, threads, sample = cpu_ensemble_sample(w, systems)
         n = sum(len(p) for p in systems)
@@ -510,6 +568,69 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
     return out
 
 
+def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
+    """The request loop in real time over the Poisson stream, for a bounded
+    wall window; value = particle-steps completed / wall time."""
+    from bhg import serve
+
+    if args.serve_budget_gb is not None:
+        w["hbm_budget_gb"] = args.serve_budget_gb
+    if args.serve_wall is not None:
+        w["wall_limit_s"] = args.serve_wall
+    if args.serve_duration is not None:
+        w["duration"] = args.serve_duration
+    reqs = serve_stream(w)
+    # warm-up: a few small requests through the same loop (kernels loaded,
+    # occupancy queried)
+    warm = serve.Server(device=rig.local, hbm_budget=2e9, max_leaf=w["max_leaf"], group_size=w["group"])
+    warm.run([serve.Request(i, 0.0, "merger" if i % 2 else "plummer", 20000, 2, 0.5, 90 + i) for i in range(3)],
+             realtime=False)
+    warm.close()
+    delivered = [0]
+
+    def on_result(rid, parts):  # the finished state goes back to the host and is dropped
+        delivered[0] += 1
+
+    srv = serve.Server(device=rig.local, hbm_budget=w["hbm_budget_gb"] * 1e9, max_leaf=w["max_leaf"],
+                       group_size=w["group"], on_result=on_result)
+    srv.ctx.stats(reset=True)
+    rig.barrier()
+    clk = ClockSampler(rig.local)
+    with clk:
+        rep = srv.run(reqs, wall_limit=w["wall_limit_s"], realtime=True)
+    rig.barrier()
+    st = srv.ctx.stats(reset=True)
+    ticks = max(1, rep["ticks"])
+    n_eval = max(1, srv.particle_evals // ticks)
+    srv.close()
+    rep["offered_requests"] = len(reqs)
+    rep["offered_particle_steps_per_s"] = sum(r.n * r.steps for r in reqs) / w["duration"]
+    rep["delivered"] = delivered[0]
+    wall = rig.max_over_ranks(rep["wall_s"])
+    ps = rep["particle_steps"] * rig.world
+    out = {"value": ps / wall, "ms_per_step": float(np.mean(srv.tick_ms)) if srv.tick_ms else None,
+           "clocks": clk.summary(), "serving": rep,
+           "latency_ms": {"p50": rep["step_latency_ms_p50"], "p99": rep["step_latency_ms_p99"],
+                          "per": "request step: wall time of the batched evaluation that advanced it"},
+           **roofline(st, n_eval, fp32_peak, peaks)}
+    out["e2e"] = {"value": ps / wall, "unit": "particle-steps/s",
+                  "h2d_bytes_per_step": int(64 * srv.system_evals / ticks),  # one 64-byte parameter record per system
+                  "d2h_bytes_per_step": int(srv.d2h_bytes / ticks),
+                  "path": "the request loop itself: requests arrive as seeds (initial conditions generated on the "
+                          "device), per-system parameters go up every tick, finished states come back to the "
+                          "host; the wall clock runs around all of it"}
+    if rig.rank == 0 and not args.no_cpu_baseline:
+        try:
+            v, threads, sample = cpu_serve_sample(w)
+            out["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                                   "sample": sample}
+        except (OSError, subprocess.CalledProcessError) as e:
+            out["cpu_baseline"] = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    out["config_extra"] = {"mean_particles_per_tick": n_eval}
+    return out
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
@@ -523,12 +644,16 @@ def main():
     if w["kind"] == "ensemble":
         res = bench_ensemble(args, w, rig, bhg, fp32_peak, peaks)
         dtype = "f32+f64"
+    elif w["kind"] == "serve":
+        res = bench_serve(args, w, rig, bhg, fp32_peak, peaks)
+        dtype = "f32+f64"
     else:
         res = bench_single(args, w, rig, bhg, fp32_peak, peaks)
         dtype = "f32+f64" if args.precision == "split" else "f64"
     if rig.rank == 0:
         cfg = {"workload": args.workload, **{k: v for k, v in w.items() if k != "kind"},
-               **res.pop("config_extra"), "precision": args.precision if w["kind"] != "ensemble" else "split",
+               **res.pop("config_extra"),
+               "precision": args.precision if w["kind"] in ("single", "merger") else "split",
                "parallelism": f"replicas x{rig.world}",
                "l2": "inputs larger than L2 (particle state, Morton copy and tree exceed 126 MB)"}
         line = {"metric": METRIC, "value": res.pop("value"), "unit": "particle-steps/s", "n_gpus": rig.world,

@@ -117,6 +117,44 @@ int bhg_download(bhg_context* ctx, bh_particle64* out);
 int bhg_download_device(bhg_context* ctx, void* out);
 size_t bhg_num_particles(const bhg_context* ctx);
 
+/* ---- systems joining and leaving (continuous batching) ---------------------
+ *
+ * The reference runs one simulation per process (main.cc:114-263); a server
+ * keeps many resident in one context instead and advances them together
+ * with bhg_step_systems.  Every system has a handle (bhg_upload* hands out
+ * new ones in order, see bhg_system_ids).  A system's results never depend
+ * on which others share the context: its tree, walk and sums only touch its
+ * own particles. */
+
+/* One Plummer sphere (scale radius a, total mass, centre, bulk velocity),
+ * G = 1, truncated at 10a: the distribution of bhg_ic_plummer. */
+typedef struct bhg_sphere {
+  uint64_t n;
+  double a;
+  double mass;
+  double centre[3];
+  double bulk[3];
+} bhg_sphere;
+
+/* Appends one system of n particles from host memory; its handle goes to
+ * *id.  The resident systems keep their particles and parameters; the new
+ * one starts with theta 0.5, eps2 0 and no kick/drift (bhg_set_system_params). */
+int bhg_add_system(bhg_context* ctx, const bh_particle64* particles, size_t n, uint64_t* id);
+/* Appends one system generated on the device: one sphere, or two (a merger)
+ * stored one after the other, particle ids id0, id0 + 1, ...  The particles
+ * come from a counter-based generator keyed by seed (the second sphere by
+ * a key derived from it), so a request's initial conditions are its seed:
+ * the same seed gives the same particles, bit for bit, on every call. */
+int bhg_add_generated(bhg_context* ctx, const bhg_sphere* spheres, int nspheres, uint64_t seed, uint32_t id0,
+                      uint64_t* id);
+/* Removes k systems by handle; out (host, optional) receives their particles
+ * back to back in the order of `handles` (blocks when given).  The others
+ * keep their order, particles and parameters. */
+int bhg_remove_systems(bhg_context* ctx, const uint64_t* handles, size_t k, bh_particle64* out);
+size_t bhg_num_systems(const bhg_context* ctx);
+/* The handles of the resident systems, in storage order (bhg_num_systems of them). */
+int bhg_system_ids(const bhg_context* ctx, uint64_t* out);
+
 /* ---- phases ---------------------------------------------------------------- */
 
 /* build_flat_tree (flat_build_ttg.h:276-281) minus the multipoles: bounds and
