@@ -87,14 +87,17 @@ class Server:
     BYTES_PER_PARTICLE each); max_leaf/group_size are the walk's sizes."""
 
     def __init__(self, device=0, hbm_budget=150e9, max_leaf=16, group_size=256, precision=PRECISION_SPLIT,
-                 keep_results=False, on_result=None):
+                 keep_results=False, on_result=None, max_batch_particles=None):
         """keep_results: store each finished request's particles in
         self.results[rid]; on_result(rid, particles): hand them to a caller
-        instead.  With neither, finished requests leave the GPU uncopied."""
+        instead.  With neither, finished requests leave the GPU uncopied.
+        max_batch_particles: a second admission cap, on the particles one
+        tick evaluates (bounds the per-step latency; None = memory only)."""
         # the context's own hard limit leaves room for its fixed tables, the
         # buffers' growth slack and the state's second copy while it grows
         self.ctx = Context(device=device, hbm_budget=int(hbm_budget * 1.15) + (512 << 20))
         self.budget = hbm_budget
+        self.max_batch = max_batch_particles
         self.max_leaf, self.group_size, self.precision = max_leaf, group_size, precision
         self.keep_results = keep_results
         self.on_result = on_result
@@ -121,8 +124,10 @@ class Server:
     def admit(self, req: Request, now: float) -> bool:
         """Adds the request to the batch if the budget allows (a request alone
         is always tried)."""
-        if self.active and (self.hold or (self._resident() + req.n) * BYTES_PER_PARTICLE > self.budget):
-            return False
+        if self.active:
+            after = self._resident() + req.n
+            if self.hold or after * BYTES_PER_PARTICLE > self.budget or (self.max_batch and after > self.max_batch):
+                return False
         try:
             h = self.ctx.add_generated(req.spheres(), req.seed, id0=0)
         except BhgError as e:

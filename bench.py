@@ -86,6 +86,8 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
     ap.add_argument("--serve-wall", type=float, default=None, help="serve: wall-clock window in seconds")
     ap.add_argument("--serve-duration", type=float, default=None, help="serve: length of the arrival stream")
+    ap.add_argument("--serve-max-batch", type=int, default=None,
+                    help="serve: also cap the particles one tick evaluates (latency-bounded batching)")
     return ap.parse_args()
 
 
@@ -579,6 +581,8 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
         w["wall_limit_s"] = args.serve_wall
     if args.serve_duration is not None:
         w["duration"] = args.serve_duration
+    if args.serve_max_batch is not None:
+        w["max_batch_particles"] = args.serve_max_batch
     reqs = serve_stream(w)
     # warm-up: a few small requests through the same loop (kernels loaded,
     # occupancy queried)
@@ -592,7 +596,8 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
         delivered[0] += 1
 
     srv = serve.Server(device=rig.local, hbm_budget=w["hbm_budget_gb"] * 1e9, max_leaf=w["max_leaf"],
-                       group_size=w["group"], on_result=on_result)
+                       group_size=w["group"], on_result=on_result,
+                       max_batch_particles=w.get("max_batch_particles"))
     srv.ctx.stats(reset=True)
     rig.barrier()
     clk = ClockSampler(rig.local)

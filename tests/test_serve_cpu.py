@@ -106,3 +106,13 @@ def test_server_schedule_kicks(monkeypatch):
     dt = 1.0 / 128
     serve.Server(hbm_budget=1e12).run([serve.Request(0, 0.0, "plummer", 1000, 3, 0.5, 7, dt=dt)], realtime=False)
     assert seen == [(dt / 2, dt), (dt, dt), (dt, dt), (dt / 2, 0.0)]
+
+
+def test_server_batch_cap(monkeypatch):
+    monkeypatch.setattr(serve, "Context", _FakeContext)
+    monkeypatch.setattr(_FakeContext, "limit", 1 << 40)
+    reqs = [serve.Request(i, 0.0, "plummer", 40_000, 2, 0.5, i) for i in range(4)]
+    srv = serve.Server(hbm_budget=1e12, max_batch_particles=100_000)
+    assert srv.admit(reqs[0], 0.0) and srv.admit(reqs[1], 0.0) and not srv.admit(reqs[2], 0.0)
+    rep = serve.Server(hbm_budget=1e12, max_batch_particles=100_000).run(reqs, realtime=False)
+    assert rep["completed"] == 4
