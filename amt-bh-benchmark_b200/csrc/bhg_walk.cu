@@ -23,18 +23,16 @@
 //
 // A walk step pops up to 32 nodes (one per lane) from a shared-memory stack;
 // accepted cells and opened leaves' particles go to two shared-memory
-// queues, and each full queue chunk is evaluated with one SOURCE PER LANE
-// against targets held in registers (up to 8 per lane; the warp splits into
-// 1-8 lane groups for up to 64 targets), so all lanes stay busy for any
-// target size.  The per-chunk bodies are specialised on the number of live
-// target slots so the independent interactions interleave.
+// queues, and a full queue is evaluated as one batch (64 cells or 128
+// particles in split precision; one source per lane against up to 2 targets
+// per lane in FP64).
 //
 // Split precision: sources and targets become FP32 offsets from the walk's
-// bounding-box centre (the subtraction in FP64), interactions are FP32 FMA
-// + rsqrtf, and every kFlushChunks chunks the FP32 partial sums are reduced
-// across the lane group into an FP64 sum owned by one lane per target
-// (compensated summation across list chunks).  The kick/drift of
-// integrate_ttg.h:74-77 is applied in FP64 in the epilogue.
+// bounding-box centre (the subtraction in FP64), staged once per batch in
+// shared memory; interactions are FP32 FMA + rsqrtf with lanes laid out as
+// (target, source subset) (SplitEval below); FP32 partials go into FP64
+// sums after every batch.  The kick/drift of integrate_ttg.h:74-77 is
+// applied in FP64 in the epilogue.
 #include "bhg_kernels.h"
 
 #include <type_traits>
@@ -43,19 +41,22 @@ namespace bhg {
 
 constexpr int kWalkWarps = 4;
 constexpr int kWalkThreads = kWalkWarps * 32;
-constexpr int kQueue = 128;  // ring of queued sources: a chunk is 2 per lane
-constexpr int kStackCap = 1280;  // per-warp shared-memory stack
-constexpr int kDeferCap = 1024;  // per-warp deferred nodes of a group walk
-constexpr int kFlushChunks = 16;
+constexpr int kCellQ = 128;   // ring of accepted cells (a batch of up to 64 + one step's 32)
+constexpr int kPartQ = 256;   // ring of direct particles (a batch of up to 128 + 32 enqueued)
+constexpr int kStackCap = 1024;  // per-warp shared-memory stack
+constexpr int kDeferCap = 512;   // per-warp deferred nodes of a group walk
+constexpr int kStageF4 = 3 * 64 + 3;  // staged source records (float4): 64 cells + the zero cell
 constexpr float kFarAway = 1.0e10f;  // padding source: contributes exactly 0
 constexpr uint32_t kFull = 0xffffffffu;
 static_assert(kStackCap >= kDeferCap + 7 * kLevels + 1 + 32, "a DFS walk from the deferred nodes must fit");
+static_assert(kStageF4 * 16 >= 32 * 6 * 8, "the end-of-walk reduction reuses the staging records");
 
 struct WarpSmem {
   uint32_t stack[kStackCap];
   uint32_t defer[kDeferCap];
-  uint32_t cell[kQueue];
-  uint32_t part[kQueue];
+  uint32_t cell[kCellQ];
+  uint32_t part[kPartQ];
+  float4 stage[kStageF4];
   double acc[kGroupMax][3];   // FP64 sum per particle of the group
   double tacc[kGroupMax][3];  // FP64 sums of one target's own walk
 };
@@ -94,195 +95,186 @@ __device__ __forceinline__ double far2(const double lo[3], const double hi[3], d
 // lane group g is target g + k * gp; lane k mod L of the group adds that
 // target's partial sums into its FP64 sum.
 
-// Split precision, up to 4 targets per lane, up to 64 per warp.
+// Split precision.  Sources are staged once per batch in shared memory as
+// FP32 records relative to the walk box's centre (the subtraction in FP64),
+// and the warp is laid out as a grid of lanes: each lane owns kt (1 or 2)
+// targets and one of ng lane groups, which split the batch's sources
+// between them (group g takes sources g, g + ng, ...).  Every lane reads
+// the records it needs from shared memory (all lanes of a group read the
+// same record: a broadcast), so a source costs one global gather per warp,
+// not one per lane group, and the lanes never exchange partial sums inside
+// a batch.  Each loop iteration evaluates two independent (source, target)
+// pairs: two sources for one target (kt = 1) or one source for two targets
+// (kt = 2).  FP32 partials are added into per-lane FP64 sums after every
+// batch; at the end of a walk the lane groups' FP64 sums are added in group
+// order (deterministic) into the targets' FP64 sums.
 template <bool QUAD, bool MASK>
 struct SplitEval {
-  static constexpr int TB = 4;
+  static constexpr int kCellBatch = 64, kPartBatch = 128;
+  static constexpr int kCellDummy = kCellBatch;  // record index of the zero cell (written once)
+  static constexpr int kPartDummy = kPartBatch;  // record index of the zero particle (written per batch)
   const WalkArgs& a;
+  float4* stage;  // records: cells 3 float4 each, particles 1 float4 each
+  double* red;    // per-lane FP64 sums at the end of a walk (aliases stage)
   double cx, cy, cz;  // reference point: the walk box's centre
   float eps2;
-  int L, gp, g, j, kmax;
-  float tx[TB], ty[TB], tz[TB];
-  float ax[TB], ay[TB], az[TB];
-  double (*acc)[3];  // FP64 sums of the targets (shared memory)
-  int ntb;
-  int chunks;
+  int lane, tb, kt, lpg, ng, first, stride, offb;
+  float t0x, t0y, t0z, t1x, t1y, t1z;  // target positions (t1 = t0 when kt = 1)
+  float a0x, a0y, a0z, a1x, a1y, a1z;  // FP32 partials of the current batch
+  double s0x, s0y, s0z, s1x, s1y, s1z;  // FP64 sums of this lane
+  double (*acc)[3];  // the targets' FP64 sums (shared memory)
 
-  __device__ explicit SplitEval(const WalkArgs& args) : a(args) {}
+  __device__ SplitEval(const WalkArgs& args, float4* stage_, int lane_) : a(args), stage(stage_), lane(lane_) {
+    red = reinterpret_cast<double*>(stage_);
+    if (lane == 0) {
+      stage[3 * kCellDummy + 0] = make_float4(kFarAway, 0.f, 0.f, 0.f);
+      stage[3 * kCellDummy + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      stage[3 * kCellDummy + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncwarp();
+  }
 
-  static __device__ int groups_for(int tb) { return tb <= 4 ? 1 : tb <= 8 ? 2 : tb <= 16 ? 4 : tb <= 32 ? 8 : 16; }
+  __device__ int cell_chunk() const { return kCellBatch; }
+  __device__ int part_chunk() const { return kPartBatch; }
 
-  // targets: particles p0 .. p0 + tb - 1 (tb <= 64); their FP64 sums are
-  // added to sums[0 .. tb)
-  __device__ void setup(int lane, uint32_t p0, int tb, double (*sums)[3]) {
+  // targets: particles p0 .. p0 + n - 1 (n <= 64); their FP64 sums are
+  // added to sums[0 .. n)
+  __device__ void setup(int, uint32_t p0, int n, double (*sums)[3]) {
     acc = sums;
-    ntb = tb;
-    gp = groups_for(tb);
-    L = 32 / gp;
-    g = lane / L;
-    j = lane & (L - 1);
-    kmax = (tb + gp - 1) / gp;
-    float p0x = 0.f, p0y = 0.f, p0z = 0.f, p1x = 0.f, p1y = 0.f, p1z = 0.f;
-    if (lane < tb) {
-      const double4 q = a.pm[p0 + lane];
-      p0x = (float)__dsub_rn(q.x, cx), p0y = (float)__dsub_rn(q.y, cy), p0z = (float)__dsub_rn(q.z, cz);
-    }
-    if (lane + 32 < tb) {
-      const double4 q = a.pm[p0 + 32 + lane];
-      p1x = (float)__dsub_rn(q.x, cx), p1y = (float)__dsub_rn(q.y, cy), p1z = (float)__dsub_rn(q.z, cz);
-    }
-#pragma unroll
-    for (int k = 0; k < TB; ++k) {
-      const int t = g + k * gp;  // < 64
-      const float x0 = __shfl_sync(kFull, p0x, t & 31), x1 = __shfl_sync(kFull, p1x, t & 31);
-      const float y0 = __shfl_sync(kFull, p0y, t & 31), y1 = __shfl_sync(kFull, p1y, t & 31);
-      const float z0 = __shfl_sync(kFull, p0z, t & 31), z1 = __shfl_sync(kFull, p1z, t & 31);
-      tx[k] = t < 32 ? x0 : x1;
-      ty[k] = t < 32 ? y0 : y1;
-      tz[k] = t < 32 ? z0 : z1;
-      ax[k] = ay[k] = az[k] = 0.f;
-    }
-    chunks = 0;
+    tb = n;
+    // one target per lane with 32 / tb lane groups, or two targets per lane
+    // with 32 / ceil(tb / 2) groups: whichever leaves fewer slots idle
+    const int n1 = tb <= 32 ? 32 / tb : 0;
+    const int l2 = (tb + 1) >> 1, n2 = 32 / l2;
+    kt = (n1 == 0 || n2 >= 2 * n1) ? 2 : 1;
+    lpg = kt == 1 ? tb : l2;
+    ng = kt == 1 ? n1 : n2;
+    const bool active = lane < lpg * ng;
+    const int slot = lane % lpg;
+    first = active ? lane / lpg : 1 << 30;  // inactive lanes take no sources
+    stride = kt == 1 ? 2 * ng : ng;
+    offb = kt == 1 ? ng : 0;
+    const int t0 = slot, t1 = (kt == 2 && slot + lpg < tb) ? slot + lpg : slot;
+    const double4 q0 = a.pm[p0 + t0], q1 = a.pm[p0 + t1];
+    t0x = (float)__dsub_rn(q0.x, cx), t0y = (float)__dsub_rn(q0.y, cy), t0z = (float)__dsub_rn(q0.z, cz);
+    t1x = (float)__dsub_rn(q1.x, cx), t1y = (float)__dsub_rn(q1.y, cy), t1z = (float)__dsub_rn(q1.z, cz);
+    a0x = a0y = a0z = a1x = a1y = a1z = 0.f;
+    s0x = s0y = s0z = s1x = s1y = s1z = 0.0;
   }
 
-  // Reduces the FP32 partial sums over the lane group and adds them to the
-  // FP64 sums; slot k of group g belongs to lane k mod L of the group.
-  __device__ void flush() {
-#pragma unroll
-    for (int k = 0; k < TB; ++k) {
-      if (k < kmax) {
-        float vx = ax[k], vy = ay[k], vz = az[k];
-        for (int o = L >> 1; o > 0; o >>= 1) {
-          vx += __shfl_xor_sync(kFull, vx, o);
-          vy += __shfl_xor_sync(kFull, vy, o);
-          vz += __shfl_xor_sync(kFull, vz, o);
-        }
-        const int t = g + k * gp;
-        if (j == (k & (L - 1)) && t < ntb) {
-          acc[t][0] += (double)vx;
-          acc[t][1] += (double)vy;
-          acc[t][2] += (double)vz;
-        }
-        ax[k] = ay[k] = az[k] = 0.f;
-      }
+  __device__ __forceinline__ void flush() {
+    s0x += (double)a0x, s0y += (double)a0y, s0z += (double)a0z;
+    if (kt == 1) {
+      s0x += (double)a1x, s0y += (double)a1y, s0z += (double)a1z;
+    } else {
+      s1x += (double)a1x, s1y += (double)a1y, s1z += (double)a1z;
     }
-    chunks = 0;
+    a0x = a0y = a0z = a1x = a1y = a1z = 0.f;
   }
 
-  __device__ __forceinline__ void tick() {
-    if (++chunks == kFlushChunks) flush();
-  }
-
-  // one source's contribution to target slot k
-  __device__ __forceinline__ void cell_one(int k, float sx, float sy, float sz, float m, const float q[6], float& rx,
-                                           float& ry, float& rz) {
-    const float dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
+  // one cell record's contribution to the target at (tx, ty, tz)
+  __device__ __forceinline__ void cell_body(const float4* r, float tx, float ty, float tz, float& ax, float& ay,
+                                            float& az) const {
+    const float4 r0 = r[0];
+    const float dx = r0.x - tx, dy = r0.y - ty, dz = r0.z - tz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
     float ri = rsqrtf(r2);
     if (!QUAD && MASK) ri = r2 > 0.f ? ri : 0.f;
     const float ri2 = ri * ri;
     const float ri3 = ri * ri2;
     if (QUAD) {
-      const float qx = fmaf(q[0], dx, fmaf(q[3], dy, q[4] * dz));
-      const float qy = fmaf(q[3], dx, fmaf(q[1], dy, q[5] * dz));
-      const float qz = fmaf(q[4], dx, fmaf(q[5], dy, q[2] * dz));
+      const float4 r1 = r[1];
+      const float2 r3 = *reinterpret_cast<const float2*>(&r[2]);
+      // Q = [[q0 q3 q4] [q3 q1 q5] [q4 q5 q2]]
+      const float qx = fmaf(r1.x, dx, fmaf(r1.w, dy, r3.x * dz));
+      const float qy = fmaf(r1.w, dx, fmaf(r1.y, dy, r3.y * dz));
+      const float qz = fmaf(r3.x, dx, fmaf(r3.y, dy, r1.z * dz));
       const float dqd = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
       const float ri5 = ri3 * ri2;
       // m d / r^3 - Q d / r^5 + 2.5 (d Q d) d / r^7
-      const float c = fmaf(2.5f * dqd, ri5 * ri2, m * ri3);
-      rx = fmaf(c, dx, -ri5 * qx);
-      ry = fmaf(c, dy, -ri5 * qy);
-      rz = fmaf(c, dz, -ri5 * qz);
+      const float c = fmaf(2.5f * dqd, ri5 * ri2, r0.w * ri3);
+      ax += fmaf(c, dx, -ri5 * qx);
+      ay += fmaf(c, dy, -ri5 * qy);
+      az += fmaf(c, dz, -ri5 * qz);
     } else {
-      const float c = m * ri3;
-      rx = c * dx, ry = c * dy, rz = c * dz;
+      const float c = r0.w * ri3;
+      ax = fmaf(c, dx, ax), ay = fmaf(c, dy, ay), az = fmaf(c, dz, az);
     }
   }
 
-  __device__ __forceinline__ void load_cell(const uint32_t* ring, uint32_t at, bool live, float& sx, float& sy,
-                                            float& sz, float& m, float q[6]) {
-    sx = kFarAway, sy = sz = m = 0.f;
-    q[0] = q[1] = q[2] = q[3] = q[4] = q[5] = 0.f;
-    if (live) {
-      const uint32_t n = ring[at & (kQueue - 1)];
-      const WNode* w = a.w + n;
-      const double2 cxy = *reinterpret_cast<const double2*>(&w->cx);
-      const double czz = w->cz;
-      sx = (float)__dsub_rn(cxy.x, cx);
-      sy = (float)__dsub_rn(cxy.y, cy);
-      sz = (float)__dsub_rn(czz, cz);
-      m = w->mass;
-      if (QUAD) {
-        const float4 qa = *reinterpret_cast<const float4*>(w->q);
-        const float2 qb = a.q45[n];
-        q[0] = qa.x, q[1] = qa.y, q[2] = qa.z, q[3] = qa.w, q[4] = qb.x, q[5] = qb.y;
-      }
-    }
-  }
-
-  // accepted cells: node ids ring[(head + i) % kQueue], i < cnt <= 2L
-  __device__ void cells(const uint32_t* ring, uint32_t head, int cnt) {
-    float s0x, s0y, s0z, m0, q0[6], s1x, s1y, s1z, m1, q1[6];
-    load_cell(ring, head + j, j < cnt, s0x, s0y, s0z, m0, q0);
-    load_cell(ring, head + L + j, L + j < cnt, s1x, s1y, s1z, m1, q1);
-#pragma unroll
-    for (int k = 0; k < TB; ++k) {
-      if (k < kmax) {
-        float ax0, ay0, az0, ax1, ay1, az1;
-        cell_one(k, s0x, s0y, s0z, m0, q0, ax0, ay0, az0);
-        cell_one(k, s1x, s1y, s1z, m1, q1, ax1, ay1, az1);
-        ax[k] += ax0 + ax1;
-        ay[k] += ay0 + ay1;
-        az[k] += az0 + az1;
-      }
-    }
-    tick();
-  }
-
-  __device__ __forceinline__ void part_one(int k, float sx, float sy, float sz, float m, float& rx, float& ry,
-                                           float& rz) {
-    const float dx = sx - tx[k], dy = sy - ty[k], dz = sz - tz[k];
+  __device__ __forceinline__ void part_body(const float4 r, float tx, float ty, float tz, float& ax, float& ay,
+                                            float& az) const {
+    const float dx = r.x - tx, dy = r.y - ty, dz = r.z - tz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
     float ri = rsqrtf(r2);
     if (MASK) ri = r2 > 0.f ? ri : 0.f;
-    const float c = m * (ri * ri) * ri;
-    rx = c * dx, ry = c * dy, rz = c * dz;
+    const float c = r.w * (ri * ri) * ri;
+    ax = fmaf(c, dx, ax), ay = fmaf(c, dy, ay), az = fmaf(c, dz, az);
   }
 
-  __device__ __forceinline__ void load_part(const uint32_t* ring, uint32_t at, bool live, float& sx, float& sy,
-                                            float& sz, float& m) {
-    sx = kFarAway, sy = sz = m = 0.f;
-    if (live) {
-      const double4 p = a.pm[ring[at & (kQueue - 1)]];
-      sx = (float)__dsub_rn(p.x, cx);
-      sy = (float)__dsub_rn(p.y, cy);
-      sz = (float)__dsub_rn(p.z, cz);
-      m = (float)p.w;
-    }
-  }
-
-  // direct particles: particle indices ring[(head + i) % kQueue], i < cnt <= 2L
-  __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
-    float s0x, s0y, s0z, m0, s1x, s1y, s1z, m1;
-    load_part(ring, head + j, j < cnt, s0x, s0y, s0z, m0);
-    load_part(ring, head + L + j, L + j < cnt, s1x, s1y, s1z, m1);
-#pragma unroll
-    for (int k = 0; k < TB; ++k) {
-      if (k < kmax) {
-        float ax0, ay0, az0, ax1, ay1, az1;
-        part_one(k, s0x, s0y, s0z, m0, ax0, ay0, az0);
-        part_one(k, s1x, s1y, s1z, m1, ax1, ay1, az1);
-        ax[k] += ax0 + ax1;
-        ay[k] += ay0 + ay1;
-        az[k] += az0 + az1;
+  // accepted cells: node ids ring[(head + i) % kCellQ], i < cnt <= kCellBatch
+  __device__ void cells(const uint32_t* ring, uint32_t head, int cnt) {
+    for (int i = lane; i < cnt; i += 32) {
+      const uint32_t n = ring[(head + (uint32_t)i) & (kCellQ - 1)];
+      const WNode* w = a.w + n;
+      const double2 cxy = *reinterpret_cast<const double2*>(&w->cx);
+      const double czz = w->cz;
+      const float4 r0 = make_float4((float)__dsub_rn(cxy.x, cx), (float)__dsub_rn(cxy.y, cy),
+                                    (float)__dsub_rn(czz, cz), w->mass);
+      stage[3 * i] = r0;
+      if (QUAD) {
+        const float4 qa = *reinterpret_cast<const float4*>(w->q);
+        const float2 qb = a.q45[n];
+        // record layout: (q0 q1 q2 q3) (q4 q5 - -)
+        stage[3 * i + 1] = qa;
+        stage[3 * i + 2] = make_float4(qb.x, qb.y, 0.f, 0.f);
       }
     }
-    tick();
+    __syncwarp();
+    for (int s = first; s < cnt; s += stride) {
+      const int sb = s + offb < cnt ? s + offb : kCellDummy;
+      cell_body(stage + 3 * s, t0x, t0y, t0z, a0x, a0y, a0z);
+      cell_body(stage + 3 * sb, t1x, t1y, t1z, a1x, a1y, a1z);
+    }
+    flush();
+    __syncwarp();
   }
 
-  // After a walk: every target's FP64 sum is complete.
-  __device__ void finish() {
+  // direct particles: particle indices ring[(head + i) % kPartQ], i < cnt <= kPartBatch
+  __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
+    for (int i = lane; i < cnt; i += 32) {
+      const double4 p = a.pm[ring[(head + (uint32_t)i) & (kPartQ - 1)]];
+      stage[i] = make_float4((float)__dsub_rn(p.x, cx), (float)__dsub_rn(p.y, cy), (float)__dsub_rn(p.z, cz),
+                             (float)p.w);
+    }
+    if (lane == 0) stage[kPartDummy] = make_float4(kFarAway, 0.f, 0.f, 0.f);
+    __syncwarp();
+    for (int s = first; s < cnt; s += stride) {
+      const int sb = s + offb < cnt ? s + offb : kPartDummy;
+      part_body(stage[s], t0x, t0y, t0z, a0x, a0y, a0z);
+      part_body(stage[sb], t1x, t1y, t1z, a1x, a1y, a1z);
+    }
     flush();
+    __syncwarp();
+  }
+
+  // After a walk: the lane groups' sums, added in group order into every
+  // target's FP64 sum.
+  __device__ void finish() {
+    if (first < (1 << 30)) {
+      double* r = red + 6 * lane;
+      r[0] = s0x, r[1] = s0y, r[2] = s0z, r[3] = s1x, r[4] = s1y, r[5] = s1z;
+    }
+    __syncwarp();
+    for (int t = lane; t < tb; t += 32) {
+      const int k = t / lpg, sl = t - k * lpg;
+      double x = 0.0, y = 0.0, z = 0.0;
+      for (int g = 0; g < ng; ++g) {
+        const double* r = red + 6 * (g * lpg + sl) + 3 * k;
+        x += r[0], y += r[1], z += r[2];
+      }
+      acc[t][0] += x, acc[t][1] += y, acc[t][2] += z;
+    }
     __syncwarp();
   }
 };
@@ -302,7 +294,10 @@ struct F64Eval {
   double (*acc)[3];
   int ntb;
 
-  __device__ explicit F64Eval(const WalkArgs& args) : a(args) {}
+  __device__ F64Eval(const WalkArgs& args, float4*, int) : a(args) {}
+
+  __device__ int cell_chunk() const { return 2 * L; }
+  __device__ int part_chunk() const { return 2 * L; }
 
   static __device__ int groups_for(int tb) {
     return tb <= 2 ? 1 : tb <= 4 ? 2 : tb <= 8 ? 4 : tb <= 16 ? 8 : tb <= 32 ? 16 : 32;
@@ -367,7 +362,7 @@ struct F64Eval {
     sx = 1.0e30, sy = sz = m = 0.0;
     q[0] = q[1] = q[2] = q[3] = q[4] = q[5] = 0.0;
     if (live) {
-      const uint32_t n = ring[at & (kQueue - 1)];
+      const uint32_t n = ring[at & (kCellQ - 1)];
       const double4 cm = a.mom[n];
       sx = cm.x, sy = cm.y, sz = cm.z, m = cm.w;
       if (QUAD) {
@@ -408,11 +403,11 @@ struct F64Eval {
   __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
     double s0x = 1.0e30, s0y = 0, s0z = 0, m0 = 0, s1x = 1.0e30, s1y = 0, s1z = 0, m1 = 0;
     if (j < cnt) {
-      const double4 p = a.pm[ring[(head + j) & (kQueue - 1)]];
+      const double4 p = a.pm[ring[(head + j) & (kPartQ - 1)]];
       s0x = p.x, s0y = p.y, s0z = p.z, m0 = p.w;
     }
     if (L + j < cnt) {
-      const double4 p = a.pm[ring[(head + L + j) & (kQueue - 1)]];
+      const double4 p = a.pm[ring[(head + L + j) & (kPartQ - 1)]];
       s1x = p.x, s1y = p.y, s1z = p.z, m1 = p.w;
     }
 #pragma unroll
@@ -469,7 +464,7 @@ template <class E>
 __device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, uint32_t nstart,
                                  const double lo[3], const double hi[3], double theta2, bool group_mode, bool dfs,
                                  int lane, unsigned long long& ncells, unsigned long long& nparts, uint32_t& ndefer) {
-  const int C = 2 * ev.L;  // sources per evaluated chunk
+  const int C = ev.cell_chunk(), CP = ev.part_chunk();  // sources per evaluated batch
   const uint32_t lt = lanemask_lt();
   uint32_t top;
   if (nstart == 0) {
@@ -501,8 +496,8 @@ __device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint3
       ncells += c;
       continue;
     }
-    if (npart >= C || (done && npart > 0)) {
-      const int c = min(npart, C);
+    if (npart >= CP || (done && npart > 0)) {
+      const int c = min(npart, CP);
       ev.parts(S.part, phead, c);
       phead += c;
       npart -= c;
@@ -523,7 +518,7 @@ __device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint3
       const uint32_t sinc = __shfl_sync(kFull, pinc, src);
       const uint32_t spc = __shfl_sync(kFull, pc, src);
       const uint32_t take = min(32u, ptot - pbase);
-      if ((uint32_t)lane < take) S.part[(phead + npart + lane) & (kQueue - 1)] = sf + (idx - (sinc - spc));
+      if ((uint32_t)lane < take) S.part[(phead + npart + lane) & (kPartQ - 1)] = sf + (idx - (sinc - spc));
       npart += take;
       pbase += take;
       __syncwarp();
@@ -559,7 +554,7 @@ __device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint3
     }
     // accepted: cell queue
     const uint32_t am = __ballot_sync(kFull, accept);
-    if (accept) S.cell[(chead + ncell + __popc(am & lt)) & (kQueue - 1)] = node;
+    if (accept) S.cell[(chead + ncell + __popc(am & lt)) & (kCellQ - 1)] = node;
     ncell += __popc(am);
     if (group_mode) {  // neither: deferred to the targets
       const bool defer = valid && !accept && !open;
@@ -673,7 +668,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;  // the build failed: touch nothing
   const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
   unsigned long long n_pp = 0, n_pc = 0;
-  E ev(a);
+  E ev(a, S.stage, lane);
   for (;;) {
     uint32_t gi = 0;
     if (lane == 0) gi = atomicAdd(&a.st->walk_next, 1u);
