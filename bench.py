@@ -94,11 +94,14 @@ def parse():
 def make_particles(w, rank=0):
     import bhg
 
+    from bhg.replicas import replica_seed
+
+    seed = replica_seed(w["seed"], rank)
     if w["kind"] == "single":
-        return bhg.plummer(w["n"], w["seed"] + rank)[0]
+        return bhg.plummer(w["n"], seed)[0]
     if w["kind"] == "merger":
-        return bhg.merger(w["n"] // 2, w["seed"] + rank)
-    return bhg.ensemble(w["nsys"], w["seed"] + rank)
+        return bhg.merger(w["n"] // 2, seed)
+    return bhg.ensemble(w["nsys"], seed)
 
 
 # ---------------------------------------------------------------------------- clocks
@@ -323,28 +326,24 @@ class Rig:
     def __init__(self):
         import torch
 
-        self.torch = torch
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        torch.cuda.set_device(self.local)
-        if self.world > 1:
-            import datetime
+        from bhg.replicas import Replicas
 
-            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        self.torch = torch
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        self.rep = Replicas("nccl", f"cuda:{local}")
+        self.world, self.rank, self.local = self.rep.world, self.rep.rank, self.rep.local
         self.stream = torch.cuda.Stream(device=self.local)
 
     def barrier(self):
         self.torch.cuda.synchronize(self.local)
-        if self.world > 1:
-            self.torch.distributed.barrier()
+        self.rep.barrier()
 
     def max_over_ranks(self, v):
-        if self.world == 1:
-            return v
-        t = self.torch.tensor([v], device=f"cuda:{self.local}")
-        self.torch.distributed.all_reduce(t, op=self.torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return self.rep.max(v)
+
+    def sum_over_ranks(self, v):
+        return self.rep.sum(v)
 
     def time_steps(self, fn, steps, warmup, after_warmup=None):
         """Device ms of `steps` calls of fn (CUDA events on the stream) and wall
@@ -445,7 +444,7 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     one_step()
     ms, wall, clocks = rig.time_steps(one_step, args.steps, max(0, args.warmup - 1), lambda: ctx.stats(reset=True))
     st = ctx.stats(reset=True)
-    ps = n * w["steps"] * args.steps * rig.world
+    ps = rig.sum_over_ranks(n * w["steps"] * args.steps)
     out = {"value": ps / (ms / 1000.0), "ms_per_step": ms / args.steps, "clocks": clocks,
            **roofline(st, n, fp32_peak, peaks)}
 
@@ -499,7 +498,7 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
     one_step()
     ms, wall, clocks = rig.time_steps(one_step, args.steps, max(0, args.warmup - 1), lambda: ctx.stats(reset=True))
     st = ctx.stats(reset=True)
-    ps = n * args.steps * rig.world
+    ps = rig.sum_over_ranks(n * args.steps)
     out = {"value": ps / (ms / 1000.0), "ms_per_step": ms / args.steps, "clocks": clocks,
            **roofline(st, n, fp32_peak, peaks),
            "autotune": {k: tuned[k] for k in ("max_leaf", "target_size", "rms_error", "err_budget", "table")}}
@@ -612,7 +611,7 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
     rep["offered_particle_steps_per_s"] = sum(r.n * r.steps for r in reqs) / w["duration"]
     rep["delivered"] = delivered[0]
     wall = rig.max_over_ranks(rep["wall_s"])
-    ps = rep["particle_steps"] * rig.world
+    ps = rig.sum_over_ranks(rep["particle_steps"])
     out = {"value": ps / wall, "ms_per_step": float(np.mean(srv.tick_ms)) if srv.tick_ms else None,
            "clocks": clk.summary(), "serving": rep,
            "latency_ms": {"p50": rep["step_latency_ms_p50"], "p99": rep["step_latency_ms_p99"],
@@ -666,9 +665,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
                 "data": "synthetic", "config": cfg, **res}
         print(json.dumps(line), flush=True)
-    if rig.world > 1:
-        rig.torch.distributed.barrier()
-        rig.torch.distributed.destroy_process_group()
+    rig.rep.close()
     return 0
 
 
