@@ -31,7 +31,8 @@ EXPORT_KEYS, EXPORT_PERM, EXPORT_NODES_U32, EXPORT_NODES_F64, EXPORT_DOMAINS, EX
 EXPORTED = (
     "bhg_create", "bhg_destroy", "bhg_last_error", "bhg_set_stream", "bhg_upload", "bhg_upload_device",
     "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_add_system",
-    "bhg_add_generated", "bhg_remove_systems", "bhg_num_systems", "bhg_system_ids", "bhg_build_tree",
+    "bhg_add_generated", "bhg_remove_systems", "bhg_num_systems", "bhg_system_ids", "bhg_upload_csv",
+    "bhg_add_csv", "bhg_snapshot_vtk", "bhg_build_tree",
     "bhg_compute_multipoles", "bhg_walk_forces", "bhg_integrate", "bhg_step", "bhg_step_systems",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
     "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
@@ -100,6 +101,9 @@ def lib() -> C.CDLL:
         "bhg_remove_systems": ([vp, vp, sz, vp], i32),
         "bhg_num_systems": ([vp], sz),
         "bhg_system_ids": ([vp, vp], i32),
+        "bhg_upload_csv": ([vp, C.c_char_p, sz], i32),
+        "bhg_add_csv": ([vp, C.c_char_p, sz, C.POINTER(u64)], i32),
+        "bhg_snapshot_vtk": ([vp, u64, C.c_char_p, sz, C.POINTER(sz)], i32),
         "bhg_build_tree": ([vp, C.c_uint, u32], i32),
         "bhg_compute_multipoles": ([vp], i32),
         "bhg_walk_forces": ([vp, C.POINTER(ForceParams), u32, f64, f64, vp, vp], i32),
@@ -246,6 +250,30 @@ class Context:
         if out is None:
             return None
         return np.split(out, np.cumsum(sizes)[:-1])
+
+    def upload_csv(self, text: bytes):
+        """The particles of a CSV text (read_csv's format), parsed on the GPU,
+        as the only system."""
+        self._ck(self.L.bhg_upload_csv(self.h, text, len(text)))
+        self.n = self.L.bhg_num_particles(self.h)
+
+    def add_csv(self, text: bytes) -> int:
+        """The same, appended as one more system; returns its handle."""
+        h = C.c_uint64()
+        self._ck(self.L.bhg_add_csv(self.h, text, len(text), C.byref(h)))
+        self.n = self.L.bhg_num_particles(self.h)
+        return h.value
+
+    def snapshot_vtk(self, handle=None) -> bytes:
+        """write_vtk's text of a system (the first when handle is None),
+        formatted on the GPU."""
+        if handle is None:
+            handle = int(self.system_ids()[0])
+        n = C.c_size_t()
+        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, buf, n.value, C.byref(n)))
+        return buf.raw[: n.value]
 
     def system_ids(self) -> np.ndarray:
         out = np.zeros(self.L.bhg_num_systems(self.h), np.uint64)

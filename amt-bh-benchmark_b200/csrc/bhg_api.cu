@@ -765,6 +765,190 @@ int bhg_remove_systems(bhg_context* c, const uint64_t* handles, size_t k, bh_par
 
 size_t bhg_num_systems(const bhg_context* c) { return c ? c->counts.size() : 0; }
 
+}  // extern "C"
+
+namespace {
+
+// Device scratch of one text operation, freed on every way out.
+struct Scratch {
+  bhg_context* c;
+  std::vector<void*> ptrs;
+  explicit Scratch(bhg_context* c_) : c(c_) {}
+  template <typename T>
+  int get(T** p, size_t count) {
+    *p = nullptr;
+    int r = dev_alloc(c, reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
+    if (r == BHG_OK) ptrs.push_back(*p);
+    return r;
+  }
+  ~Scratch() {
+    for (void* p : ptrs) dev_free(c, p);
+  }
+};
+
+// read_csv's header rule (io.cc:136-141): the first line is a header when its
+// first field (after blanks) does not parse as an id.
+bool csv_has_header(const char* text, size_t n) {
+  const char* end = text + n;
+  const char* eol = static_cast<const char*>(std::memchr(text, '\n', n));
+  const char* lim = eol ? eol : end;
+  const char* p = text;
+  while (p < lim && (*p == ' ' || *p == '\t')) ++p;
+  uint64_t v = 0;
+  const char* q = p;
+  while (q < lim && *q >= '0' && *q <= '9') {
+    v = v * 10 + (uint64_t)(*q - '0');
+    if (v > 0xffffffffull) return true;
+    ++q;
+  }
+  return q == p;
+}
+
+// Parses CSV text (host memory) on the device: *n_kept particle lines;
+// *tmp/*keep/*m stay allocated in `sc` for the compaction.
+int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, Particle** tmp, uint32_t** keep,
+              uint64_t* m, uint64_t* n_kept) {
+  cudaStream_t s = c->stream;
+  char* dtext = nullptr;
+  uint32_t* tiles = nullptr;
+  uint64_t* totals = nullptr;
+  uint64_t* line_start = nullptr;
+  unsigned long long* bad = nullptr;
+  int r;
+  if ((r = sc.get(&dtext, nbytes)) || (r = sc.get(&tiles, csv_tiles(nbytes))) || (r = sc.get(&totals, 2)) ||
+      (r = sc.get(&bad, 1)))
+    return r;
+  if (nbytes) CK(cudaMemcpyAsync(dtext, text, nbytes, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(totals, 0, 2 * sizeof(uint64_t), s));
+  CK(cudaMemsetAsync(bad, 0xff, sizeof(unsigned long long), s));
+  launch_csv_count(dtext, nbytes, tiles, totals, s);
+  CK(cudaGetLastError());
+  uint64_t h[2] = {0, 0};
+  CK(cudaMemcpyAsync(h, totals, sizeof h, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const uint64_t nlines = h[0] + 1;
+  if ((r = sc.get(&line_start, nlines))) return r;
+  CK(cudaMemsetAsync(line_start, 0, sizeof(uint64_t), s));
+  launch_csv_emit(dtext, nbytes, tiles, line_start, s);
+  const uint64_t first = (nbytes && csv_has_header(text, nbytes)) ? 1 : 0;
+  *m = nlines > first ? nlines - first : 0;
+  uint32_t* block_count = nullptr;
+  if ((r = sc.get(tmp, *m)) || (r = sc.get(keep, *m)) || (r = sc.get(&block_count, csv_keep_blocks(*m)))) return r;
+  launch_csv_parse(dtext, nbytes, line_start, first, nlines, *tmp, *keep, bad, c->sms, s);
+  launch_csv_compact(*tmp, *keep, *m, block_count, totals + 1, nullptr, s);
+  CK(cudaGetLastError());
+  unsigned long long hb = 0;
+  CK(cudaMemcpyAsync(&hb, bad, sizeof hb, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(h, totals, sizeof h, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (hb != ~0ull) {  // the first malformed line, as read_csv reports it
+    uint64_t ls[2] = {0, nbytes + 1};
+    CK(cudaMemcpy(ls, line_start + hb, (hb + 1 < nlines ? 2 : 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    const size_t b = (size_t)ls[0], e = std::min<size_t>((size_t)ls[1] - 1, nbytes);
+    return fail(c, BHG_EINVAL, "malformed line " + std::to_string(hb + 1) + ": '" + std::string(text + b, text + e) + "'");
+  }
+  *n_kept = h[1];
+  return BHG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bhg_upload_csv(bhg_context* c, const char* text, size_t nbytes) {
+  if (!c) return BHG_EINVAL;
+  if (!text && nbytes) return fail(c, BHG_EINVAL, "null text");
+  cudaSetDevice(c->device);
+  Scratch sc(c);
+  Particle* tmp = nullptr;
+  uint32_t* keep = nullptr;
+  uint64_t m = 0, n = 0;
+  int r = csv_parse(c, sc, text, nbytes, &tmp, &keep, &m, &n);
+  if (r) return r;
+  if (n == 0) return fail(c, BHG_EINVAL, "no particles in the text");
+  const uint64_t cnt = n;
+  if ((r = set_problem(c, &cnt, 1))) return r;
+  uint32_t* block_count = nullptr;
+  uint64_t* total = nullptr;
+  if ((r = sc.get(&block_count, csv_keep_blocks(m))) || (r = sc.get(&total, 1))) return r;
+  launch_csv_compact(tmp, keep, m, block_count, total, c->part, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return BHG_OK;
+}
+
+int bhg_add_csv(bhg_context* c, const char* text, size_t nbytes, uint64_t* id) {
+  if (!c) return BHG_EINVAL;
+  if (!text && nbytes) return fail(c, BHG_EINVAL, "null text");
+  cudaSetDevice(c->device);
+  Scratch sc(c);
+  Particle* tmp = nullptr;
+  uint32_t* keep = nullptr;
+  uint64_t m = 0, n = 0;
+  int r = csv_parse(c, sc, text, nbytes, &tmp, &keep, &m, &n);
+  if (r) return r;
+  if (n == 0) return fail(c, BHG_EINVAL, "no particles in the text");
+  uint32_t* block_count = nullptr;
+  uint64_t* total = nullptr;
+  if ((r = sc.get(&block_count, csv_keep_blocks(m))) || (r = sc.get(&total, 1))) return r;
+  r = add_system_impl(c, n, id, [&](Particle* dst) -> int {
+    launch_csv_compact(tmp, keep, m, block_count, total, dst, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return BHG_OK;
+  });
+  return r;
+}
+
+int bhg_snapshot_vtk(bhg_context* c, uint64_t handle, char* out, size_t cap, size_t* len) {
+  if (!c || !len) return BHG_EINVAL;
+  cudaSetDevice(c->device);
+  auto it = std::find(c->ids.begin(), c->ids.end(), handle);
+  if (it == c->ids.end()) return fail(c, BHG_EINVAL, "no system with handle " + std::to_string(handle));
+  const size_t sidx = (size_t)(it - c->ids.begin());
+  size_t start = 0;
+  for (size_t k = 0; k < sidx; ++k) start += c->counts[k];
+  const uint32_t n = (uint32_t)c->counts[sidx];
+  Scratch sc(c);
+  char* slots = nullptr;
+  uint32_t* lens = nullptr;
+  uint64_t* offs = nullptr;
+  uint64_t* totals = nullptr;
+  int r;
+  if ((r = sc.get(&slots, vtk_slot_bytes(n))) || (r = sc.get(&lens, 3 * (size_t)n)) ||
+      (r = sc.get(&offs, 3 * (size_t)n)) || (r = sc.get(&totals, 3)))
+    return r;
+  launch_vtk_format(c->part + start, n, slots, lens, offs, totals, c->sms, c->stream);
+  CK(cudaGetLastError());
+  uint64_t t[3];
+  CK(cudaMemcpyAsync(t, totals, sizeof t, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // write_vtk's layout (io.cc:180-195)
+  const std::string h0 = "# vtk DataFile Version 3.0\npepc-ttg particle snapshot\nASCII\nDATASET POLYDATA\nPOINTS " +
+                         std::to_string(n) + " double\n";
+  const std::string h1 = "POINT_DATA " + std::to_string(n) + "\nSCALARS mass double 1\nLOOKUP_TABLE default\n";
+  const std::string h2 = "VECTORS velocity double\n";
+  const size_t total = h0.size() + t[0] + h1.size() + t[1] + h2.size() + t[2];
+  *len = total;
+  if (!out) return BHG_OK;
+  if (cap < total) return fail(c, BHG_EINVAL, "buffer too small: the snapshot needs " + std::to_string(total) + " bytes");
+  char* dev = nullptr;
+  if ((r = sc.get(&dev, t[0] + t[1] + t[2]))) return r;
+  char* sect[3] = {dev, dev + t[0], dev + t[0] + t[1]};
+  launch_vtk_gather(slots, n, lens, offs, sect, c->sms, c->stream);
+  CK(cudaGetLastError());
+  const std::string* head[3] = {&h0, &h1, &h2};
+  size_t at = 0;
+  for (int k = 0; k < 3; ++k) {
+    std::memcpy(out + at, head[k]->data(), head[k]->size());
+    at += head[k]->size();
+    if (t[k]) CK(cudaMemcpyAsync(out + at, sect[k], t[k], cudaMemcpyDeviceToHost, c->stream));
+    at += t[k];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return BHG_OK;
+}
+
 int bhg_system_ids(const bhg_context* c, uint64_t* out) {
   if (!c || !out) return BHG_EINVAL;
   std::copy(c->ids.begin(), c->ids.end(), out);

@@ -67,6 +67,27 @@ void launch_direct(const double4* pm, uint32_t begin, uint32_t n, const uint32_t
                    double G, double* out, cudaStream_t s);
 void launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int sms, cudaStream_t s);
 double measure_fp32_peak(int device);
+// Particle text (bhg_csv.cu).  Ingest: newline count per 16 KB tile and the
+// scan of the tile counts (total newlines to *total), then the line starts
+// (newlines + 1 of them), then one parse per line of [first, nlines), then
+// the compaction of the particle lines (kept count to *total; dst may be
+// null to count only).  Snapshot: formats the three text lines of every
+// particle into slots (lengths, exclusive offsets and the three section
+// totals), then gathers each section back to back.
+size_t csv_tiles(size_t nbytes);
+void launch_csv_count(const char* text, size_t n, uint32_t* tile_count, uint64_t* total, cudaStream_t s);
+void launch_csv_emit(const char* text, size_t n, const uint32_t* tile_off, uint64_t* line_start, cudaStream_t s);
+void launch_csv_parse(const char* text, size_t n, const uint64_t* line_start, uint64_t first, uint64_t nlines,
+                      Particle* tmp, uint32_t* keep, unsigned long long* bad, int sms, cudaStream_t s);
+size_t csv_keep_blocks(uint64_t m);
+void launch_csv_compact(const Particle* tmp, const uint32_t* keep, uint64_t m, uint32_t* block_count,
+                        uint64_t* total, Particle* dst, cudaStream_t s);
+size_t vtk_slot_bytes(uint32_t n);
+void launch_vtk_format(const Particle* p, uint32_t n, char* slots, uint32_t* len, uint64_t* off, uint64_t* totals,
+                       int sms, cudaStream_t s);
+void launch_vtk_gather(const char* slots, uint32_t n, const uint32_t* len, const uint64_t* off, char* const out[3],
+                       int sms, cudaStream_t s);
+
 // n particles of one Plummer sphere (scale a, total mass `mass`, centre c[3],
 // bulk velocity b[3], ids id0..), drawn from a counter-based generator keyed
 // by `seed`.

@@ -152,6 +152,29 @@ int bhg_add_generated(bhg_context* ctx, const bhg_sphere* spheres, int nspheres,
  * keep their order, particles and parameters. */
 int bhg_remove_systems(bhg_context* ctx, const uint64_t* handles, size_t k, bh_particle64* out);
 size_t bhg_num_systems(const bhg_context* ctx);
+
+/* ---- particle text on the device ----------------------------------------------
+ *
+ * read_csv (io.cc:122-178) and write_vtk (io.cc:180-195), done by the GPU:
+ * the text crosses PCIe once and is parsed or written by kernels, bit for bit
+ * as the reference reads and writes it. */
+
+/* Parses CSV text (host memory, nbytes bytes; one particle per line:
+ * id,mass,x,y,z,vx,vy,vz; blanks around fields, an optional '\r' at line
+ * ends, blank lines skipped, an optional header line whose first field is not
+ * an id, numbers converted exactly as std::from_chars does) and makes the
+ * particles the context's only system, in file order.  A malformed line gives
+ * BHG_EINVAL with the line number and text in bhg_last_error.  Replaces
+ * read_csv + bhg_upload. */
+int bhg_upload_csv(bhg_context* ctx, const char* text, size_t nbytes);
+/* The same, appended as one more system (handle to *id). */
+int bhg_add_csv(bhg_context* ctx, const char* text, size_t nbytes, uint64_t* id);
+/* The system `handle` as write_vtk writes it (legacy VTK ASCII PolyData:
+ * points, mass scalar, velocity vector; numbers as an ostream with default
+ * settings writes them), in storage order.  *len receives the size in bytes;
+ * out (host, cap bytes) receives the text unless it is NULL; a buffer smaller
+ * than *len gives BHG_EINVAL.  Blocks until done. */
+int bhg_snapshot_vtk(bhg_context* ctx, uint64_t handle, char* out, size_t cap, size_t* len);
 /* The handles of the resident systems, in storage order (bhg_num_systems of them). */
 int bhg_system_ids(const bhg_context* ctx, uint64_t* out);
 

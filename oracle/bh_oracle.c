@@ -25,6 +25,7 @@
  * contract a*b+c, so plain IEEE operations reproduce its rounding.
  */
 #include <math.h>
+#include <stdio.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -620,4 +621,185 @@ int bho_step(bho_particle* p, const uint32_t* seg_begin, const uint32_t* seg_n, 
   free(dom), free(keys), free(skeys), free(perm), free(tmp), free(x), free(u), free(dd), free(targets), free(roots),
       free(tfp), free(acc);
   return 0;
+}
+
+/* ---- particle text: read_csv (io.cc:70-178) and write_vtk (io.cc:180-195) ----
+ *
+ * The numbers follow std::from_chars(double, general): the grammar is checked
+ * here and the value comes from the C library's strtod on exactly the
+ * accepted characters (glibc's strtod is correctly rounded, as from_chars is);
+ * a nonzero value that rounds to zero or to infinity is out of range. */
+
+static const char* bho_skip_blanks(const char* p, const char* end) {
+  while (p < end && (*p == ' ' || *p == '\t')) ++p;
+  return p;
+}
+
+static int bho_lower(int c) { return c | 0x20; }
+
+/* end of the from_chars number at p (p itself when there is none) */
+static const char* bho_number_end(const char* p, const char* end, int* nonzero, int* special) {
+  const char* s = p;
+  *nonzero = 0;
+  *special = 0;
+  if (s < end && *s == '-') ++s;
+  if (s + 3 <= end && bho_lower(s[0]) == 'i' && bho_lower(s[1]) == 'n' && bho_lower(s[2]) == 'f') {
+    s += 3;
+    if (s + 5 <= end && bho_lower(s[0]) == 'i' && bho_lower(s[1]) == 'n' && bho_lower(s[2]) == 'i' &&
+        bho_lower(s[3]) == 't' && bho_lower(s[4]) == 'y')
+      s += 5;
+    *special = 1;
+    return s;
+  }
+  if (s + 3 <= end && bho_lower(s[0]) == 'n' && bho_lower(s[1]) == 'a' && bho_lower(s[2]) == 'n') {
+    s += 3;
+    if (s < end && *s == '(') {
+      const char* t = s + 1;
+      while (t < end && ((*t >= '0' && *t <= '9') || (bho_lower(*t) >= 'a' && bho_lower(*t) <= 'z') || *t == '_')) ++t;
+      if (t < end && *t == ')') s = t + 1;
+    }
+    *special = 1;
+    return s;
+  }
+  int digits = 0;
+  while (s < end && *s >= '0' && *s <= '9') digits++, *nonzero |= *s != '0', ++s;
+  if (s < end && *s == '.') {
+    ++s;
+    while (s < end && *s >= '0' && *s <= '9') digits++, *nonzero |= *s != '0', ++s;
+  }
+  if (!digits) return p;
+  if (s < end && bho_lower(*s) == 'e') {
+    const char* t = s + 1;
+    if (t < end && (*t == '+' || *t == '-')) ++t;
+    if (t < end && *t >= '0' && *t <= '9') {
+      while (t < end && *t >= '0' && *t <= '9') ++t;
+      s = t;
+    }
+  }
+  return s;
+}
+
+/* parse_field (io.cc:76-91) for a double; 0 on success */
+static int bho_field_f64(const char** pp, const char* end, double* out, int last) {
+  const char* p = bho_skip_blanks(*pp, end);
+  int nonzero, special;
+  const char* q = bho_number_end(p, end, &nonzero, &special);
+  if (q == p) return 1;
+  char buf[1100];
+  char* heap = NULL;
+  char* tmp = buf;
+  const size_t len = (size_t)(q - p);
+  if (len + 1 > sizeof buf) tmp = heap = (char*)malloc(len + 1);
+  memcpy(tmp, p, len);
+  tmp[len] = 0;
+  const double v = strtod(tmp, NULL);
+  free(heap);
+  if (!special && (isinf(v) || (v == 0.0 && nonzero))) return 1; /* result_out_of_range */
+  *out = v;
+  q = bho_skip_blanks(q, end);
+  if (last) {
+    if (q < end && *q == '\r') ++q;
+    if (q != end) return 1;
+  } else {
+    if (q >= end || *q != ',') return 1;
+    ++q;
+  }
+  *pp = q;
+  return 0;
+}
+
+/* the id field: from_chars into uint32 */
+static int bho_field_id(const char** pp, const char* end, uint32_t* out) {
+  const char* p = bho_skip_blanks(*pp, end);
+  const char* q = p;
+  uint64_t v = 0;
+  while (q < end && *q >= '0' && *q <= '9') {
+    v = v * 10 + (uint64_t)(*q - '0');
+    if (v > 0xffffffffull) return 1;
+    ++q;
+  }
+  if (q == p) return 1;
+  *out = (uint32_t)v;
+  q = bho_skip_blanks(q, end);
+  if (q >= end || *q != ',') return 1;
+  *pp = q + 1;
+  return 0;
+}
+
+/* read_csv of a text in memory.  Returns 0 with *n particles (those beyond
+ * cap are counted, not stored), or 1 with *bad_line the 0-based number of the
+ * first malformed line. */
+int bho_read_csv(const char* text, size_t nbytes, bho_particle* out, size_t cap, size_t* n, size_t* bad_line) {
+  const char* begin = text;
+  const char* end = text + nbytes;
+  size_t line_no = 0;
+  *n = 0;
+  if (begin == end) return 0;
+  { /* header: the first field of the first line is not an id (io.cc:136-141) */
+    const char* eol = (const char*)memchr(begin, '\n', nbytes);
+    const char* lim = eol ? eol : end;
+    const char* p = bho_skip_blanks(begin, lim);
+    const char* q = p;
+    uint64_t v = 0;
+    int over = 0;
+    while (q < lim && *q >= '0' && *q <= '9') {
+      v = v * 10 + (uint64_t)(*q - '0');
+      if (v > 0xffffffffull) over = 1;
+      ++q;
+    }
+    if (q == p || over) begin = eol ? eol + 1 : end, line_no = 1;
+  }
+  for (const char* line = begin; line < end; ++line_no) { /* parse_lines, io.cc:95-113 */
+    const char* eol = (const char*)memchr(line, '\n', (size_t)(end - line));
+    if (!eol) eol = end;
+    const char* p = bho_skip_blanks(line, eol);
+    if (p != eol && *p != '\r') {
+      bho_particle q;
+      memset(&q, 0, sizeof q);
+      if (bho_field_id(&p, eol, &q.id) || bho_field_f64(&p, eol, &q.mass, 0) || bho_field_f64(&p, eol, &q.pos[0], 0) ||
+          bho_field_f64(&p, eol, &q.pos[1], 0) || bho_field_f64(&p, eol, &q.pos[2], 0) ||
+          bho_field_f64(&p, eol, &q.vel[0], 0) || bho_field_f64(&p, eol, &q.vel[1], 0) ||
+          bho_field_f64(&p, eol, &q.vel[2], 1)) {
+        *bad_line = line_no;
+        return 1;
+      }
+      if (*n < cap) out[*n] = q;
+      ++*n;
+    }
+    line = eol + 1;
+  }
+  return 0;
+}
+
+/* write_vtk's text (numbers as printf "%g"); returns its length and writes
+ * min(length, cap) bytes to out */
+size_t bho_write_vtk(const bho_particle* p, size_t n, char* out, size_t cap) {
+  size_t len = 0;
+  char buf[160];
+#define BHO_PUT(s, k)                                         \
+  do {                                                        \
+    const size_t k_ = (size_t)(k);                            \
+    if (len < cap) memcpy(out + len, s, len + k_ <= cap ? k_ : cap - len); \
+    len += k_;                                                \
+  } while (0)
+  int k = snprintf(buf, sizeof buf,
+                   "# vtk DataFile Version 3.0\npepc-ttg particle snapshot\nASCII\nDATASET POLYDATA\nPOINTS %zu double\n", n);
+  BHO_PUT(buf, k);
+  for (size_t i = 0; i < n; ++i) {
+    k = snprintf(buf, sizeof buf, "%g %g %g\n", p[i].pos[0], p[i].pos[1], p[i].pos[2]);
+    BHO_PUT(buf, k);
+  }
+  k = snprintf(buf, sizeof buf, "POINT_DATA %zu\nSCALARS mass double 1\nLOOKUP_TABLE default\n", n);
+  BHO_PUT(buf, k);
+  for (size_t i = 0; i < n; ++i) {
+    k = snprintf(buf, sizeof buf, "%g\n", p[i].mass);
+    BHO_PUT(buf, k);
+  }
+  BHO_PUT("VECTORS velocity double\n", 24);
+  for (size_t i = 0; i < n; ++i) {
+    k = snprintf(buf, sizeof buf, "%g %g %g\n", p[i].vel[0], p[i].vel[1], p[i].vel[2]);
+    BHO_PUT(buf, k);
+  }
+#undef BHO_PUT
+  return len;
 }

@@ -67,6 +67,10 @@ class Oracle:
         L.bho_potential.restype = f64
         L.bho_step.argtypes = [vp, vp, vp, sz, vp, vp, vp, C.c_uint, u32, u32, vp, vp]
         L.bho_step.restype = C.c_int
+        L.bho_read_csv.argtypes = [C.c_char_p, sz, vp, sz, C.POINTER(sz), C.POINTER(sz)]
+        L.bho_read_csv.restype = C.c_int
+        L.bho_write_vtk.argtypes = [vp, sz, C.c_char_p, sz]
+        L.bho_write_vtk.restype = sz
 
     # -- pieces ---------------------------------------------------------
     def domain(self, parts: np.ndarray) -> tuple[np.ndarray, int]:
@@ -149,6 +153,25 @@ class Oracle:
         self.lib.bho_direct(_p(x), _p(y), _p(z), _p(m), len(x), _p(idx), len(idx), eps2, G, _p(out))
         return out
 
+    def read_csv(self, text: bytes):
+        """read_csv (io.cc:122-178) of a text in memory: (particles, None), or
+        (None, 0-based number of the first malformed line)."""
+        n, bad = C.c_size_t(), C.c_size_t()
+        cap = text.count(b"\n") + 1
+        out = np.zeros(cap, PARTICLE)
+        r = self.lib.bho_read_csv(text, len(text), _p(out), cap, C.byref(n), C.byref(bad))
+        if r:
+            return None, bad.value
+        return out[: n.value].copy(), None
+
+    def write_vtk(self, parts) -> bytes:
+        """write_vtk (io.cc:180-195) as bytes."""
+        parts = np.ascontiguousarray(parts, dtype=PARTICLE)
+        need = self.lib.bho_write_vtk(_p(parts), len(parts), None, 0)
+        buf = C.create_string_buffer(need)
+        self.lib.bho_write_vtk(_p(parts), len(parts), buf, need)
+        return buf.raw[:need]
+
     def kinetic(self, parts) -> float:
         parts = np.ascontiguousarray(parts, dtype=PARTICLE)
         return self.lib.bho_kinetic(_p(parts), len(parts))
@@ -216,6 +239,45 @@ class Reference:
         L.bhref_kinetic.restype = f64
         L.bhref_potential.argtypes = [vp, sz, f64]
         L.bhref_potential.restype = f64
+        L.bhref_read_csv.argtypes = [C.c_char_p, vp, sz, C.POINTER(sz), C.c_char_p, sz]
+        L.bhref_read_csv.restype = C.c_int
+        L.bhref_write_vtk.argtypes = [C.c_char_p, vp, sz]
+        L.bhref_write_vtk.restype = C.c_int
+
+    def read_csv(self, text: bytes):
+        """The reference's read_csv on a temporary file holding `text`:
+        (particles, None) or (None, the exception's message)."""
+        import tempfile
+
+        with tempfile.NamedTemporaryFile(suffix=".csv", delete=False) as f:
+            f.write(text)
+            path = f.name
+        try:
+            cap = text.count(b"\n") + 1
+            out = np.zeros(cap, PARTICLE)
+            n = C.c_size_t()
+            err = C.create_string_buffer(4096)
+            r = self.lib.bhref_read_csv(path.encode(), _p(out), cap, C.byref(n), err, 4096)
+        finally:
+            os.unlink(path)
+        if r:
+            return None, err.value.decode(errors="replace")
+        return out[: n.value].copy(), None
+
+    def write_vtk(self, parts) -> bytes:
+        """The reference's write_vtk, read back as bytes."""
+        import tempfile
+
+        parts = np.ascontiguousarray(parts, dtype=PARTICLE)
+        with tempfile.NamedTemporaryFile(suffix=".vtk", delete=False) as f:
+            path = f.name
+        try:
+            if self.lib.bhref_write_vtk(path.encode(), _p(parts), len(parts)):
+                raise RuntimeError("write_vtk threw")
+            with open(path, "rb") as f:
+                return f.read()
+        finally:
+            os.unlink(path)
 
     def build(self, parts, max_leaf, group_size) -> dict:
         parts = np.ascontiguousarray(parts, dtype=PARTICLE)

@@ -14,9 +14,11 @@
 #include "grouped_ttg.h"
 #include "integrate.h"
 #include "integrate_ttg.h"
+#include "io.h"
 
 #include <ttg.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -176,6 +178,33 @@ void bhref_accel_from_source(const double* target, double mass, const double* co
 }
 
 double bhref_kinetic(const void* particles, std::size_t n) { return bh::kinetic_energy(to_vec(particles, n)); }
+
+// read_csv (io.cc): 0 and the particles (up to cap) with their count, or 1
+// and the exception's message in err.
+int bhref_read_csv(const char* path, void* out, std::size_t cap, std::size_t* n, char* err, std::size_t errcap) {
+  try {
+    const std::vector<bh::Particle> v = bh::read_csv(path);
+    *n = v.size();
+    std::memcpy(out, v.data(), std::min(cap, v.size()) * sizeof(bh::Particle));
+    return 0;
+  } catch (const std::exception& e) {
+    if (errcap) {
+      std::strncpy(err, e.what(), errcap - 1);
+      err[errcap - 1] = 0;
+    }
+    return 1;
+  }
+}
+
+// write_vtk (io.cc) of n particles to path.
+int bhref_write_vtk(const char* path, const void* particles, std::size_t n) {
+  try {
+    bh::write_vtk(path, to_vec(particles, n));
+    return 0;
+  } catch (const std::exception&) {
+    return 1;
+  }
+}
 double bhref_potential(const void* particles, std::size_t n, double G) {
   return bh::potential_energy(to_vec(particles, n), G);
 }
