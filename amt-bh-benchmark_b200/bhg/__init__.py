@@ -32,7 +32,7 @@ EXPORTED = (
     "bhg_create", "bhg_destroy", "bhg_last_error", "bhg_set_stream", "bhg_upload", "bhg_upload_device",
     "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_add_system",
     "bhg_add_generated", "bhg_remove_systems", "bhg_num_systems", "bhg_system_ids", "bhg_upload_csv",
-    "bhg_add_csv", "bhg_snapshot_vtk", "bhg_build_tree",
+    "bhg_upload_csv_device", "bhg_add_csv", "bhg_snapshot_vtk", "bhg_build_tree",
     "bhg_compute_multipoles", "bhg_walk_forces", "bhg_integrate", "bhg_step", "bhg_step_systems",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
     "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
         "bhg_num_systems": ([vp], sz),
         "bhg_system_ids": ([vp, vp], i32),
         "bhg_upload_csv": ([vp, C.c_char_p, sz], i32),
+        "bhg_upload_csv_device": ([vp, vp, sz], i32),
         "bhg_add_csv": ([vp, C.c_char_p, sz, C.POINTER(u64)], i32),
         "bhg_snapshot_vtk": ([vp, u64, C.c_char_p, sz, C.POINTER(sz)], i32),
         "bhg_build_tree": ([vp, C.c_uint, u32], i32),
@@ -255,6 +256,11 @@ class Context:
         """The particles of a CSV text (read_csv's format), parsed on the GPU,
         as the only system."""
         self._ck(self.L.bhg_upload_csv(self.h, text, len(text)))
+        self.n = self.L.bhg_num_particles(self.h)
+
+    def upload_csv_device(self, ptr: int, nbytes: int):
+        """upload_csv for text at a device address of this context's GPU."""
+        self._ck(self.L.bhg_upload_csv_device(self.h, C.c_void_p(ptr), nbytes))
         self.n = self.L.bhg_num_particles(self.h)
 
     def add_csv(self, text: bytes) -> int:

@@ -59,6 +59,7 @@ struct bhg_context {
   uint32_t *level_lb = nullptr, *mark = nullptr, *targets = nullptr, *scan_lb = nullptr;
   uint32_t *groups = nullptr, *group_first = nullptr;
   double* accel = nullptr;
+  std::vector<std::pair<void*, size_t>> text_scratch;  // cached buffers of the text calls
   DevState* st = nullptr;
   DevState* st_host = nullptr;  // pinned
 
@@ -770,19 +771,27 @@ size_t bhg_num_systems(const bhg_context* c) { return c ? c->counts.size() : 0; 
 namespace {
 
 // Device scratch of one text operation, freed on every way out.
+// Device scratch of one text operation: the k-th buffer a call asks for is
+// the context's k-th cached buffer, grown when too small and kept for the
+// next call (repeated ingests allocate nothing).
 struct Scratch {
   bhg_context* c;
-  std::vector<void*> ptrs;
+  size_t k = 0;
   explicit Scratch(bhg_context* c_) : c(c_) {}
   template <typename T>
   int get(T** p, size_t count) {
-    *p = nullptr;
-    int r = dev_alloc(c, reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
-    if (r == BHG_OK) ptrs.push_back(*p);
-    return r;
-  }
-  ~Scratch() {
-    for (void* p : ptrs) dev_free(c, p);
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (k == c->text_scratch.size()) c->text_scratch.push_back({nullptr, 0});
+    auto& slot = c->text_scratch[k++];
+    if (slot.second < bytes) {
+      dev_free(c, slot.first);
+      slot = {nullptr, 0};
+      int r = dev_alloc(c, &slot.first, bytes);
+      if (r) return r;
+      slot.second = bytes;
+    }
+    *p = static_cast<T*>(slot.first);
+    return BHG_OK;
   }
 };
 
@@ -804,10 +813,11 @@ bool csv_has_header(const char* text, size_t n) {
   return q == p;
 }
 
-// Parses CSV text (host memory) on the device: *n_kept particle lines;
-// *tmp/*keep/*m stay allocated in `sc` for the compaction.
-int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, Particle** tmp, uint32_t** keep,
-              uint64_t* m, uint64_t* n_kept) {
+// Parses CSV text (host memory, or device memory when on_device) on the
+// device: *n_kept particle lines; *tmp/*keep/*m stay allocated in `sc` for
+// the compaction.
+int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, bool on_device, Particle** tmp,
+              uint32_t** keep, uint64_t* m, uint64_t* n_kept) {
   cudaStream_t s = c->stream;
   char* dtext = nullptr;
   uint32_t* tiles = nullptr;
@@ -815,10 +825,18 @@ int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, Part
   uint64_t* line_start = nullptr;
   unsigned long long* bad = nullptr;
   int r;
-  if ((r = sc.get(&dtext, nbytes)) || (r = sc.get(&tiles, csv_tiles(nbytes))) || (r = sc.get(&totals, 2)) ||
-      (r = sc.get(&bad, 1)))
+  if ((!on_device && (r = sc.get(&dtext, nbytes))) || (r = sc.get(&tiles, csv_tiles(nbytes))) ||
+      (r = sc.get(&totals, 2)) || (r = sc.get(&bad, 1)))
     return r;
-  if (nbytes) CK(cudaMemcpyAsync(dtext, text, nbytes, cudaMemcpyHostToDevice, s));
+  // the header rule needs the first line only
+  std::string head;
+  if (on_device) {
+    dtext = const_cast<char*>(text);
+    head.resize(std::min<size_t>(nbytes, 65536));
+    if (!head.empty()) CK(cudaMemcpyAsync(&head[0], text, head.size(), cudaMemcpyDeviceToHost, s));
+  } else if (nbytes) {
+    CK(cudaMemcpyAsync(dtext, text, nbytes, cudaMemcpyHostToDevice, s));
+  }
   CK(cudaMemsetAsync(totals, 0, 2 * sizeof(uint64_t), s));
   CK(cudaMemsetAsync(bad, 0xff, sizeof(unsigned long long), s));
   launch_csv_count(dtext, nbytes, tiles, totals, s);
@@ -830,7 +848,8 @@ int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, Part
   if ((r = sc.get(&line_start, nlines))) return r;
   CK(cudaMemsetAsync(line_start, 0, sizeof(uint64_t), s));
   launch_csv_emit(dtext, nbytes, tiles, line_start, s);
-  const uint64_t first = (nbytes && csv_has_header(text, nbytes)) ? 1 : 0;
+  const uint64_t first =
+      nbytes && (on_device ? csv_has_header(head.data(), head.size()) : csv_has_header(text, nbytes)) ? 1 : 0;
   *m = nlines > first ? nlines - first : 0;
   uint32_t* block_count = nullptr;
   if ((r = sc.get(tmp, *m)) || (r = sc.get(keep, *m)) || (r = sc.get(&block_count, csv_keep_blocks(*m)))) return r;
@@ -845,7 +864,9 @@ int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, Part
     uint64_t ls[2] = {0, nbytes + 1};
     CK(cudaMemcpy(ls, line_start + hb, (hb + 1 < nlines ? 2 : 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     const size_t b = (size_t)ls[0], e = std::min<size_t>((size_t)ls[1] - 1, nbytes);
-    return fail(c, BHG_EINVAL, "malformed line " + std::to_string(hb + 1) + ": '" + std::string(text + b, text + e) + "'");
+    std::string line(e > b ? std::min<size_t>(e - b, 4096) : 0, '\0');
+    if (!line.empty()) CK(cudaMemcpy(&line[0], dtext + b, line.size(), cudaMemcpyDeviceToHost));
+    return fail(c, BHG_EINVAL, "malformed line " + std::to_string(hb + 1) + ": '" + line + "'");
   }
   *n_kept = h[1];
   return BHG_OK;
@@ -855,7 +876,7 @@ int csv_parse(bhg_context* c, Scratch& sc, const char* text, size_t nbytes, Part
 
 extern "C" {
 
-int bhg_upload_csv(bhg_context* c, const char* text, size_t nbytes) {
+static int upload_csv_impl(bhg_context* c, const char* text, size_t nbytes, bool on_device) {
   if (!c) return BHG_EINVAL;
   if (!text && nbytes) return fail(c, BHG_EINVAL, "null text");
   cudaSetDevice(c->device);
@@ -863,7 +884,7 @@ int bhg_upload_csv(bhg_context* c, const char* text, size_t nbytes) {
   Particle* tmp = nullptr;
   uint32_t* keep = nullptr;
   uint64_t m = 0, n = 0;
-  int r = csv_parse(c, sc, text, nbytes, &tmp, &keep, &m, &n);
+  int r = csv_parse(c, sc, text, nbytes, on_device, &tmp, &keep, &m, &n);
   if (r) return r;
   if (n == 0) return fail(c, BHG_EINVAL, "no particles in the text");
   const uint64_t cnt = n;
@@ -877,6 +898,12 @@ int bhg_upload_csv(bhg_context* c, const char* text, size_t nbytes) {
   return BHG_OK;
 }
 
+int bhg_upload_csv(bhg_context* c, const char* text, size_t nbytes) { return upload_csv_impl(c, text, nbytes, false); }
+
+int bhg_upload_csv_device(bhg_context* c, const void* text, size_t nbytes) {
+  return upload_csv_impl(c, static_cast<const char*>(text), nbytes, true);
+}
+
 int bhg_add_csv(bhg_context* c, const char* text, size_t nbytes, uint64_t* id) {
   if (!c) return BHG_EINVAL;
   if (!text && nbytes) return fail(c, BHG_EINVAL, "null text");
@@ -885,7 +912,7 @@ int bhg_add_csv(bhg_context* c, const char* text, size_t nbytes, uint64_t* id) {
   Particle* tmp = nullptr;
   uint32_t* keep = nullptr;
   uint64_t m = 0, n = 0;
-  int r = csv_parse(c, sc, text, nbytes, &tmp, &keep, &m, &n);
+  int r = csv_parse(c, sc, text, nbytes, false, &tmp, &keep, &m, &n);
   if (r) return r;
   if (n == 0) return fail(c, BHG_EINVAL, "no particles in the text");
   uint32_t* block_count = nullptr;

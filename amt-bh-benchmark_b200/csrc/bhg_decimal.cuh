@@ -205,8 +205,10 @@ BHG_HD int parse_double(const char* first, const char* last, double* out, const 
     }
     return kInvalid;
   }
-  // significant digits go into w in chunks of 9
+  // significant digits go into w in chunks of 9 (and, while they fit, into
+  // w64 for the 128-bit fast path)
   big_set(w, 0);
+  uint64_t w64 = 0;
   int ndig = 0, chunk_len = 0;
   uint32_t chunk = 0;
   bool any = false, sticky = false;
@@ -225,6 +227,7 @@ BHG_HD int parse_double(const char* first, const char* last, double* out, const 
         continue;
       }
       if (ndig < kMaxDigits) {
+        if (ndig < 19) w64 = w64 * 10 + c;
         chunk = chunk * 10 + c;
         if (++chunk_len == 9) {
           big_mul_add(w, pow10[9], chunk);
@@ -263,37 +266,73 @@ BHG_HD int parse_double(const char* first, const char* last, double* out, const 
   // value = q_int * 2^e + (a fraction, and the sticky bit) with q_int of 55-57 bits
   uint64_t q;
   int e;
-  if (exp10 >= 0) {
-    big_mul_pow5(w, (int)exp10);  // value = w * 2^exp10
-    const int bl = big_bitlen(w);
-    if (bl <= 57) {
-      q = big_low64(w) << (57 - bl);
-      e = (int)exp10 - (57 - bl);
-    } else {
-      const int sh = bl - 57;
-      // the top 57 bits, the rest into the sticky bit
-      for (int i = 0; i < (sh >> 5); ++i)
-        if (w.d[i]) sticky = true;
-      if (sh & 31)
-        if (w.d[sh >> 5] & ((1u << (sh & 31)) - 1u)) sticky = true;
-      uint64_t v = 0;
-      for (int i = 0; i < 57; ++i) {
-        const int bit = sh + i;
-        if ((w.d[bit >> 5] >> (bit & 31)) & 1u) v |= 1ull << i;
+  bool fast = false;
+  if (ndig <= 19 && !sticky && exp10 >= -27 && exp10 <= 27) {
+    // fast path: w and 5^|exp10| (< 2^63) fit in 64 bits, the product or
+    // the scaled dividend in 128
+    uint64_t p5 = 1;
+    for (long i = 0; i < (exp10 < 0 ? -exp10 : exp10); ++i) p5 *= 5u;
+    if (exp10 >= 0) {
+      const unsigned __int128 N = (unsigned __int128)w64 * p5;  // value = N * 2^exp10
+      int bl = 0;
+      for (unsigned __int128 v = N; v; v >>= 1) ++bl;
+      if (bl <= 57) {
+        q = (uint64_t)N << (57 - bl);
+        e = (int)exp10 - (57 - bl);
+      } else {
+        const int sh = bl - 57;
+        q = (uint64_t)(N >> sh);
+        if (N & ((((unsigned __int128)1) << sh) - 1u)) sticky = true;
+        e = (int)exp10 + sh;
       }
-      q = v;
-      e = (int)exp10 + sh;
+      fast = true;
+    } else {
+      int blw = 0, bld = 0;
+      for (uint64_t v = w64; v; v >>= 1) ++blw;
+      for (uint64_t v = p5; v; v >>= 1) ++bld;
+      const int t = 56 + bld - blw;  // value = (w64 * 2^t / p5) * 2^(exp10 - t)
+      if (t >= 0) {
+        const unsigned __int128 N = (unsigned __int128)w64 << t;  // below 2^(56 + bld) <= 2^119
+        q = (uint64_t)(N / p5);
+        if (N % p5) sticky = true;
+        e = (int)exp10 - t;
+        fast = true;
+      }
     }
-  } else {
-    const int k = (int)-exp10;  // value = w / (5^k * 2^k)
-    big_set(b, 1);
-    big_mul_pow5(b, k);
-    int t = 56 + big_bitlen(b) - big_bitlen(w);
-    if (t >= 0) big_shl(w, t);
-    else big_shl(b, -t);
-    q = big_divmod(w, b, 58);  // below 2^57
-    if (w.n) sticky = true;
-    e = -k - t;
+  }
+  if (!fast) {
+    if (exp10 >= 0) {
+      big_mul_pow5(w, (int)exp10);  // value = w * 2^exp10
+      const int bl = big_bitlen(w);
+      if (bl <= 57) {
+        q = big_low64(w) << (57 - bl);
+        e = (int)exp10 - (57 - bl);
+      } else {
+        const int sh = bl - 57;
+        // the top 57 bits, the rest into the sticky bit
+        for (int i = 0; i < (sh >> 5); ++i)
+          if (w.d[i]) sticky = true;
+        if (sh & 31)
+          if (w.d[sh >> 5] & ((1u << (sh & 31)) - 1u)) sticky = true;
+        uint64_t v = 0;
+        for (int i = 0; i < 57; ++i) {
+          const int bit = sh + i;
+          if ((w.d[bit >> 5] >> (bit & 31)) & 1u) v |= 1ull << i;
+        }
+        q = v;
+        e = (int)exp10 + sh;
+      }
+    } else {
+      const int k = (int)-exp10;  // value = w / (5^k * 2^k)
+      big_set(b, 1);
+      big_mul_pow5(b, k);
+      int t = 56 + big_bitlen(b) - big_bitlen(w);
+      if (t >= 0) big_shl(w, t);
+      else big_shl(b, -t);
+      q = big_divmod(w, b, 58);  // below 2^57
+      if (w.n) sticky = true;
+      e = -k - t;
+    }
   }
   // round q * 2^e (+ sticky) to a double
   int bq = 0;

@@ -27,6 +27,11 @@ Other workloads (--workload):
                 150 GB HBM admission budget; reports p50/p99 per-step latency
                 and aggregate particle-steps/s over a bounded wall window
                 (120 s; --steps/--warmup do not apply)
+  csv-4m        particle text ingest (read_csv on the GPU): the 4M Plummer
+                sphere of configs[1] as CSV (%.17g numbers, ~330 MB); one step =
+                one bhg_upload_csv_device of the text resident in HBM; metric
+                particles/s (e2e: bhg_upload_csv from pinned host memory);
+                CPU baseline: the reference's own read_csv (all host threads)
   plummer-1m    a smaller case of configs[1] for profiler captures
 
 --impl reference times the reference's own CPU implementation of the path
@@ -62,6 +67,7 @@ WORKLOADS = {
                        group=256, dt=1.0 / 256, steps=8),
     "ensemble-512": dict(kind="ensemble", nsys=512, seed=3, theta=0.5, eps=0.01, max_leaf=16, target=16, group=256,
                          dt=1.0 / 128, steps=32),
+    "csv-4m": dict(kind="csv", n=4194304, seed=2),
     "serve-200rps": dict(kind="serve", rate=200.0, duration=60.0, seed=5, nmin=4096, nmax=2097152, smin=16,
                          smax=256, thetas=(0.4, 0.5, 0.7), eps=0.01, dt=1.0 / 128, max_leaf=16, target=16,
                          group=256, hbm_budget_gb=150.0, wall_limit_s=120.0),
@@ -569,6 +575,84 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
     return out
 
 
+def bench_csv(args, w, rig, bhg, peaks):
+    """read_csv on the GPU: the CSV text of the workload's particles, parsed
+    into the context's state each step."""
+    import ctypes
+
+    torch = rig.torch
+    parts, _ = bhg.plummer(w["n"], w["seed"])
+    with tempfile.NamedTemporaryFile(suffix=".csv", delete=False) as f:
+        path = f.name
+    try:
+        bhg.write_csv(path, parts)
+        text = open(path, "rb").read()
+    finally:
+        os.unlink(path)
+    nb = len(text)
+    dev = torch.frombuffer(bytearray(text), dtype=torch.uint8).to(f"cuda:{rig.local}")
+    ctx = bhg.Context(device=rig.local)
+    ctx.set_stream(rig.stream.cuda_stream)
+
+    def one_step():
+        ctx.upload_csv_device(dev.data_ptr(), nb)
+
+    ms, wall, clocks = rig.time_steps(one_step, args.steps, args.warmup)
+    n = w["n"]
+    assert ctx.n == n and ctx.download().tobytes() == parts.tobytes()  # the text round-trips exactly
+    ps = rig.sum_over_ranks(n * args.steps)
+    algo = nb + 64 * n  # text read once, particles written once
+    hbm = peaks.get("hbm_gbs")
+    gbs = algo / (ms / args.steps / 1000.0) / 1e9
+    out = {"value": ps / (ms / 1000.0), "ms_per_step": ms / args.steps, "clocks": clocks,
+           "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                        "frac": gbs / hbm if hbm else None, "traffic": None,
+                        "kernel": "the whole ingest (newline count/scan/emit, k_csv_parse, compaction)",
+                        "bytes_model": "text bytes + 64 B per particle"},
+           "gpu_launches": 9 * args.steps}
+    if not args.no_e2e:
+        pin = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+        pin.numpy()[:] = np.frombuffer(text, np.uint8)
+        addr = ctypes.c_char_p(pin.data_ptr())
+
+        def e2e_step():
+            ctx._ck(ctx.L.bhg_upload_csv(ctx.h, addr, nb))
+
+        ems, _, _ = rig.time_steps(e2e_step, args.steps, 1)
+        out["e2e"] = {"value": ps / (ems / 1000.0), "unit": "particles/s", "h2d_bytes_per_step": nb,
+                      "d2h_bytes_per_step": 0, "path": "bhg_upload_csv from pinned host memory"}
+    ctx.close()
+    if rig.rank == 0 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            from oracle import Reference
+
+            ref = Reference()
+            with tempfile.NamedTemporaryFile(suffix=".csv", delete=False) as f:
+                f.write(text)
+                path = f.name
+            try:
+                cap = n + 1
+                buf = np.zeros(cap, bhg.PARTICLE)
+                cnt = ctypes.c_size_t()
+                err = ctypes.create_string_buffer(256)
+                ref.lib.bhref_read_csv(path.encode(), buf.ctypes.data, cap, ctypes.byref(cnt), err, 256)  # warm
+                t0 = time.perf_counter()
+                ref.lib.bhref_read_csv(path.encode(), buf.ctypes.data, cap, ctypes.byref(cnt), err, 256)
+                dt = time.perf_counter() - t0
+            finally:
+                os.unlink(path)
+            out["cpu_baseline"] = {"value": n / dt, "unit": "particles/s", "cores": os.cpu_count(),
+                                   "kind": "reference",
+                                   "sample": f"the full text ({nb} bytes) through the reference's read_csv (mmap + one "
+                                             f"thread per usable CPU), after one untimed read"}
+        except (OSError, AttributeError) as e:
+            out["cpu_baseline"] = {"value": None, "unit": "particles/s", "cores": None, "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    out["config_extra"] = {"text_bytes": nb, "number_format": "%.17g"}
+    return out
+
+
 def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
     """The request loop in real time over the Poisson stream, for a bounded
     wall window; value = particle-steps completed / wall time."""
@@ -651,6 +735,9 @@ def main():
     elif w["kind"] == "serve":
         res = bench_serve(args, w, rig, bhg, fp32_peak, peaks)
         dtype = "f32+f64"
+    elif w["kind"] == "csv":
+        res = bench_csv(args, w, rig, bhg, peaks)
+        dtype = "u8->f64"
     else:
         res = bench_single(args, w, rig, bhg, fp32_peak, peaks)
         dtype = "f32+f64" if args.precision == "split" else "f64"
@@ -660,7 +747,8 @@ def main():
                "precision": args.precision if w["kind"] in ("single", "merger") else "split",
                "parallelism": f"replicas x{rig.world}",
                "l2": "inputs larger than L2 (particle state, Morton copy and tree exceed 126 MB)"}
-        line = {"metric": METRIC, "value": res.pop("value"), "unit": "particle-steps/s", "n_gpus": rig.world,
+        metric, unit = (METRIC, "particle-steps/s") if w["kind"] != "csv" else ("csv-ingest particles/s", "particles/s")
+        line = {"metric": metric, "value": res.pop("value"), "unit": unit, "n_gpus": rig.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
                 "data": "synthetic", "config": cfg, **res}

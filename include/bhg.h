@@ -167,6 +167,8 @@ size_t bhg_num_systems(const bhg_context* ctx);
  * BHG_EINVAL with the line number and text in bhg_last_error.  Replaces
  * read_csv + bhg_upload. */
 int bhg_upload_csv(bhg_context* ctx, const char* text, size_t nbytes);
+/* The same for text already in device memory of the context's GPU. */
+int bhg_upload_csv_device(bhg_context* ctx, const void* text, size_t nbytes);
 /* The same, appended as one more system (handle to *id). */
 int bhg_add_csv(bhg_context* ctx, const char* text, size_t nbytes, uint64_t* id);
 /* The system `handle` as write_vtk writes it (legacy VTK ASCII PolyData:
