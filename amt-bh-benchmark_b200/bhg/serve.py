@@ -41,6 +41,8 @@ class Request:
     seed: int
     eps: float = 0.01
     dt: float = 1.0 / 128
+    text: bytes | None = None  # initial conditions as CSV (read_csv's format) instead of a generator
+    snapshot: bool = False  # return the final state as write_vtk's text
 
     def spheres(self):
         """The request's initial conditions as device-generated spheres: one
@@ -105,6 +107,7 @@ class Server:
         self.particle_evals = 0  # resident particles summed over ticks
         self.system_evals = 0  # resident systems summed over ticks
         self.results = {}
+        self.snapshots = {}  # request id -> write_vtk text of its final state
         self.active: list[_Active] = []
         self.requeue: list[Request] = []
         self.tick_ms: list[float] = []
@@ -129,7 +132,10 @@ class Server:
             if self.hold or after * BYTES_PER_PARTICLE > self.budget or (self.max_batch and after > self.max_batch):
                 return False
         try:
-            h = self.ctx.add_generated(req.spheres(), req.seed, id0=0)
+            if req.text is not None:  # parsed on the device
+                h = self.ctx.add_csv(req.text)
+            else:
+                h = self.ctx.add_generated(req.spheres(), req.seed, id0=0)
         except BhgError as e:
             if e.code == ENOMEM and self.active:  # no room until some request leaves
                 return False
@@ -195,6 +201,9 @@ class Server:
             if a.evals_done == a.req.steps + 1:
                 done.append(a)
         if done:
+            for a in done:  # snapshots are formatted on the device before the systems leave
+                if a.req.snapshot:
+                    self.snapshots[a.req.rid] = self.ctx.snapshot_vtk(a.handle)
             want = self.keep_results or self.on_result is not None
             parts = self.ctx.remove_systems([a.handle for a in done], want=want, sizes=[a.req.n for a in done])
             for j, a in enumerate(done):

@@ -126,3 +126,30 @@ def test_add_beyond_budget_leaves_the_resident_systems():
         ref.upload(sysA)
         ref.step(fp, 16, 256, 16, 0.01, 0.01)
         assert ref.download().tobytes() == got.tobytes()
+
+
+def test_text_request_served_with_snapshot(oracle):
+    """A request whose initial state arrives as CSV text (parsed on the device)
+    and whose final state leaves as a VTK snapshot (formatted on the device)
+    ends where the same text stepped alone ends."""
+    from text_cases import csv_text
+
+    parts, _ = bhg.plummer(6000, 21)
+    text = csv_text(parts, 3, styles=(0, 1))
+    treq = serve.Request(100, 0.0, "plummer", len(parts), 3, 0.6, 0, text=text, snapshot=True)
+    others = [serve.Request(i, 0.0, "merger", 5000, 2 + i, 0.5, 40 + i) for i in range(3)]
+    srv = serve.Server(hbm_budget=1e10, keep_results=True)
+    rep = srv.run([others[0], treq, *others[1:]], realtime=False)
+    srv.close()
+    assert rep["completed"] == 4
+    with bhg.Context(device=0) as ctx:
+        ctx.upload_csv(text)
+        fp = bhg.Context.params(0.5, treq.eps ** 2, 1.0, True, bhg.PRECISION_SPLIT)
+        for e in range(treq.steps + 1):
+            kick = treq.dt / 2 if e in (0, treq.steps) else treq.dt
+            drift = 0.0 if e == treq.steps else treq.dt
+            ctx.set_system_params(theta=[treq.theta], eps2=[treq.eps ** 2], kick_dt=[kick], drift_dt=[drift])
+            ctx.step_systems(fp, G_MAX_LEAF, G_GROUP, G_MAX_LEAF)
+        alone = ctx.download()
+    assert srv.results[100].tobytes() == alone.tobytes()
+    assert srv.snapshots[100] == oracle.write_vtk(alone)
