@@ -84,6 +84,15 @@ class _Active:
     counted: int = 0  # particle-steps credited so far
 
 
+@dataclasses.dataclass
+class Checkpoint:
+    """A request's state between two evaluations: its particles (storage
+    order) and how far along its schedule it is."""
+    particles: np.ndarray
+    evals_done: int
+    counted: int
+
+
 class Server:
     """The request loop.  hbm_budget caps the admitted particles (about
     BYTES_PER_PARTICLE each); max_leaf/group_size are the walk's sizes."""
@@ -117,6 +126,9 @@ class Server:
         self.admitted = 0
         self.preempted = 0
         self.hold = False  # after a preemption: admit nothing until a request completes
+        self.saved: dict[int, Checkpoint] = {}  # suspended requests, resumed at their next admission
+        self.cancelled: set[int] = set()
+        self.n_cancelled = 0
 
     def close(self):
         self.ctx.close()
@@ -131,8 +143,11 @@ class Server:
             after = self._resident() + req.n
             if self.hold or after * BYTES_PER_PARTICLE > self.budget or (self.max_batch and after > self.max_batch):
                 return False
+        ck = self.saved.get(req.rid)
         try:
-            if req.text is not None:  # parsed on the device
+            if ck is not None:  # resumed where it was suspended
+                h = self.ctx.add_system(ck.particles)
+            elif req.text is not None:  # parsed on the device
                 h = self.ctx.add_csv(req.text)
             else:
                 h = self.ctx.add_generated(req.spheres(), req.seed, id0=0)
@@ -140,21 +155,43 @@ class Server:
             if e.code == ENOMEM and self.active:  # no room until some request leaves
                 return False
             raise
-        self.active.append(_Active(req, h, 0, now))
-        self.admitted += 1
+        if ck is not None:
+            del self.saved[req.rid]
+            self.active.append(_Active(req, h, ck.evals_done, now, ck.counted))
+        else:
+            self.active.append(_Active(req, h, 0, now))
+            self.admitted += 1
         return True
 
+    def suspend(self, rid) -> Checkpoint:
+        """Takes an admitted request off the GPU with its state; it resumes
+        from that state (not from its seed) when it is admitted again, which
+        run() does as soon as memory allows."""
+        a = next(x for x in self.active if x.req.rid == rid)
+        parts = self.ctx.remove_systems([a.handle], want=True, sizes=[a.req.n])[0]
+        self.active = [x for x in self.active if x is not a]
+        ck = Checkpoint(parts, a.evals_done, a.counted)
+        self.saved[rid] = ck
+        self.requeue.append(a.req)
+        return ck
+
+    def cancel(self, rid):
+        """Drops a request: off the GPU if admitted, never admitted if queued."""
+        self.cancelled.add(rid)
+        for a in self.active:
+            if a.req.rid == rid:
+                self.ctx.remove_systems([a.handle])
+                self.active = [x for x in self.active if x is not a]
+                self.n_cancelled += 1
+                break
+        self.saved.pop(rid, None)
+
     def _preempt(self):
-        """Sends the most recently admitted request back to the queue; it
-        starts again from its seed when it is admitted next."""
-        a = self.active.pop()
-        self.ctx.remove_systems([a.handle])
-        self.particle_steps -= a.counted
-        self._lat = [x for x in self._lat if x[0] != a.req.rid]
-        self.admitted -= 1
+        """Suspends the most recently admitted request (its state is kept and
+        it resumes from there) and holds admission until a request completes."""
+        self.suspend(self.active[-1].req.rid)
         self.preempted += 1
         self.hold = True
-        self.requeue.append(a.req)
 
     def tick(self):
         """One evaluation of every admitted request; retires the finished ones.
@@ -233,6 +270,10 @@ class Server:
             while self.requeue:
                 pending.append(self.requeue.pop())
             while pending and (not realtime or pending[-1].arrival <= now):
+                if pending[-1].rid in self.cancelled:
+                    pending.pop()
+                    self.n_cancelled += 1
+                    continue
                 if not self.admit(pending[-1], now):
                     break
                 pending.pop()
@@ -255,6 +296,7 @@ class Server:
         lat = np.array(self.step_latency_ms) if self._lat else np.zeros(1)
         return {"wall_s": wall_s, "admitted": self.admitted, "completed": self.completed,
                 "in_flight": len(self.active), "queued": queued, "preempted": self.preempted,
+                "cancelled": self.n_cancelled,
                 "ticks": len(self.tick_ms), "particle_steps": self.particle_steps,
                 "particle_steps_per_s": self.particle_steps / wall_s if wall_s > 0 else 0.0,
                 "step_latency_ms_p50": float(np.percentile(lat, 50)),

@@ -3,6 +3,8 @@
 #include "bhg.h"
 #include "bhg_kernels.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -424,8 +426,18 @@ void fold_times(bhg_context* c) {
 
 // Runs `enq` as phase `phase`: from a captured graph when `graphed`, with a
 // CUDA event before and after it on the stream.
+// NVTX range names of the phases (host-side enqueue ranges; a profiler shows
+// the kernels under them)
+const char* const kPhaseName[kPhases] = {"bhg pre", "bhg sort", "bhg tree", "bhg moments", "bhg targets", "bhg walk"};
+
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
 template <typename F>
 int run_phase(bhg_context* c, int phase, bool graphed, const std::string& key, F enq) {
+  const NvtxRange range(kPhaseName[phase]);
   if (c->pending.size() > 16384) fold_times(c);
   if (!c->open_ev) {
     c->open_ev = take_event(c);

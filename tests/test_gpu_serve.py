@@ -153,3 +153,23 @@ def test_text_request_served_with_snapshot(oracle):
         alone = ctx.download()
     assert srv.results[100].tobytes() == alone.tobytes()
     assert srv.snapshots[100] == oracle.write_vtk(alone)
+
+
+@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
+def test_suspended_request_resumes_bit_for_bit(precision):
+    """Suspend (state to the host) and resume (state back as a new system)
+    in the middle of the schedule: the request ends where it ends without
+    the interruption."""
+    reqs = [serve.Request(i, 0.0, "merger" if i % 2 else "plummer", 6000 + 1000 * i, 4, 0.5, 500 + i)
+            for i in range(3)]
+    srv = serve.Server(hbm_budget=1e10, keep_results=True, precision=precision)
+    for r in reqs:
+        srv.admit(r, 0.0)
+    srv.tick(), srv.tick()
+    srv.suspend(1)
+    srv.tick()  # the others move on without it
+    rep = srv.run([], realtime=False)
+    srv.close()
+    assert rep["completed"] == 3
+    for r in reqs:
+        assert srv.results[r.rid].tobytes() == run_alone(r, precision).tobytes()

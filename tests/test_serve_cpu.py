@@ -56,9 +56,17 @@ class _FakeContext:
         if sum(self.sizes.values()) > self.limit:
             raise serve.BhgError(serve.ENOMEM, "device out of memory")
 
+    def add_system(self, parts):
+        h = self.next
+        self.next += 1
+        self.sizes[h] = len(parts)
+        return h
+
     def remove_systems(self, handles, want=False, sizes=None):
+        out = [np.zeros(self.sizes[h]) for h in handles] if want else None
         for h in handles:
             del self.sizes[h]
+        return out
 
     def close(self):
         pass
@@ -116,3 +124,34 @@ def test_server_batch_cap(monkeypatch):
     assert srv.admit(reqs[0], 0.0) and srv.admit(reqs[1], 0.0) and not srv.admit(reqs[2], 0.0)
     rep = serve.Server(hbm_budget=1e12, max_batch_particles=100_000).run(reqs, realtime=False)
     assert rep["completed"] == 4
+
+
+def test_suspended_request_resumes_where_it_stopped(monkeypatch):
+    monkeypatch.setattr(serve, "Context", _FakeContext)
+    monkeypatch.setattr(_FakeContext, "limit", 1 << 40)
+    reqs = [serve.Request(i, 0.0, "plummer", 1000 * (i + 1), 5, 0.5, i) for i in range(3)]
+    srv = serve.Server(hbm_budget=1e12)
+    for r in reqs:
+        srv.admit(r, 0.0)
+    srv.tick(), srv.tick()
+    ck = srv.suspend(1)
+    assert ck.evals_done == 2 and len(ck.particles) == 2000 and len(srv.active) == 2
+    rep = srv.run([], realtime=False)  # the suspended request is resumed, not restarted
+    assert rep["completed"] == 3
+    assert rep["particle_steps"] == sum(r.n * r.steps for r in reqs)
+    assert len(srv.step_latency_ms) == sum(r.steps for r in reqs)
+
+
+def test_cancel_active_and_queued(monkeypatch):
+    monkeypatch.setattr(serve, "Context", _FakeContext)
+    monkeypatch.setattr(_FakeContext, "limit", 1 << 40)
+    reqs = [serve.Request(i, 0.0, "plummer", 1000, 4, 0.5, i) for i in range(4)]
+    budget = 2.5 * 1000 * serve.BYTES_PER_PARTICLE  # two at a time
+    srv = serve.Server(hbm_budget=budget)
+    srv.admit(reqs[0], 0.0), srv.admit(reqs[1], 0.0)
+    srv.tick()
+    srv.cancel(0)  # admitted
+    srv.cancel(3)  # still queued
+    rep = srv.run(reqs[2:], realtime=False)
+    assert rep["cancelled"] == 2 and rep["completed"] == 2
+    assert srv.ctx.sizes == {}
