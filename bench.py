@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 Barnes-Hut hot path (one JSON line on rank 0).
 
-Default workload: one Plummer sphere, N = 4,194,304
+Default workload (plummer-4m): one Plummer sphere, N = 4,194,304
 (seed 2, G = M = a = 1), theta 0.5, eps 0.005, monopole + quadrupole,
 max_leaf 16, target 16, group 256, advanced by the reference's leapfrog
 schedule for 8 KDK steps of dt = 1/256 (main.cc:199-246: 9 force
@@ -9,17 +9,17 @@ evaluations).  One bench step = that whole 8-step sequence over the
 GPU-resident particles; metric particle-steps/s = N * 8 * steps / time.
 
 Other workloads (--workload):
-  plummer-65k   configs[0]: N = 65,536, seed 1, eps 0.01, dt 1/128, 16 steps
-  merger-16m    configs[2]: two Plummer spheres of 8,388,608 (a = 1 and 0.5,
+  plummer-65k   N = 65,536, seed 1, eps 0.01, dt 1/128, 16 steps
+  merger-16m    two Plummer spheres of 8,388,608 (a = 1 and 0.5,
                 centres x = -5 / +5, approaching at 0.3), theta 0.6,
                 eps 0.002, dt 1/256, 8 steps
-  ensemble-512  configs[3]: 512 independent Plummer systems, N log-uniform in
+  ensemble-512  512 independent Plummer systems, N log-uniform in
                 [1,024, 262,144] (seed 3), eps 0.01, dt 1/128; one bench step
                 = one lockstep KDK evaluation of every system, batched in one
                 segmented key space, split precision, leaf/target sizes from
                 the autotuner; also times the plain FP64 path looping over
-                the systems one at a time (the north-star comparison)
-  serve-200rps  configs[4]: Poisson arrivals at 200 requests/s for 60 s, each
+                the systems one at a time (the batched-vs-plain comparison)
+  serve-200rps  Poisson arrivals at 200 requests/s for 60 s, each
                 a Plummer sphere or a merger (50/50), N log-uniform in
                 [4,096, 2,097,152], 16-256 steps, theta from {0.4, 0.5, 0.7},
                 eps 0.01, dt 1/128, generated on the device from a
@@ -28,11 +28,11 @@ Other workloads (--workload):
                 and aggregate particle-steps/s over a bounded wall window
                 (120 s; --steps/--warmup do not apply)
   csv-4m        particle text ingest (read_csv on the GPU): the 4M Plummer
-                sphere of configs[1] as CSV (%.17g numbers, ~330 MB); one step =
+                sphere of plummer-4m as CSV (%.17g numbers, 639 MB); one step =
                 one bhg_upload_csv_device of the text resident in HBM; metric
                 particles/s (e2e: bhg_upload_csv from pinned host memory);
                 CPU baseline: the reference's own read_csv (all host threads)
-  plummer-1m    a smaller case of configs[1] for profiler captures
+  plummer-1m    plummer-4m at N = 1,048,576, one KDK step, for profiler captures
 
 --impl reference times the reference's own CPU implementation of the path
 (oracle/_ref/ref_bench: the unmodified reference sources with a thread-pool

@@ -4,7 +4,7 @@ the C ABI.  Integer results (keys, order, topology) and the FP64 build
 the stated tolerances:
 
   FP64 walk   vs oracle walk: global relative error <= 1e-12
-  split walk  vs oracle walk: global relative error <= 1e-5 (north-star gate)
+  split walk  vs oracle walk: global relative error <= 1e-5 (the split-precision gate)
   theta = 0   vs direct sum:  <= 1e-8 (FP64) / 1e-5 (split), as
               test_bh_vs_bruteforce.cc:55-76 requires of the reference
 """
