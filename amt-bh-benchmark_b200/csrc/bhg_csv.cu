@@ -137,8 +137,9 @@ __device__ bool field_id(const char*& p, const char* end, uint32_t& out) {
   return true;
 }
 
-// parse_field for a double
-__device__ bool field_f64(const char*& p, const char* end, double& out, bool last, dec::Big& w, dec::Big& b) {
+// parse_field for a double (one out-of-line copy: the conversion is large,
+// and seven inlined copies would not stay in the instruction cache)
+__device__ __noinline__ bool field_f64(const char*& p, const char* end, double& out, bool last, dec::Big& w, dec::Big& b) {
   p = skip_blanks(p, end);
   const char* q;
   if (dec::parse_double(p, end, &out, &q, w, b) != dec::kOk) return false;
