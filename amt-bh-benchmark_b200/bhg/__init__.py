@@ -275,11 +275,13 @@ class Context:
         formatted on the GPU."""
         if handle is None:
             handle = int(self.system_ids()[0])
+        # one call, into a buffer of the largest possible size: three lines of
+        # at most 98 bytes per particle, plus the headers
+        cap = 98 * int(self.n) + 512
+        buf = np.empty(cap, np.uint8)
         n = C.c_size_t()
-        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, None, 0, C.byref(n)))
-        buf = C.create_string_buffer(n.value)
-        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, buf, n.value, C.byref(n)))
-        return buf.raw[: n.value]
+        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, buf.ctypes.data_as(C.c_char_p), cap, C.byref(n)))
+        return buf[: n.value].tobytes()
 
     def system_ids(self) -> np.ndarray:
         out = np.zeros(self.L.bhg_num_systems(self.h), np.uint64)

@@ -951,13 +951,14 @@ int bhg_snapshot_vtk(bhg_context* c, uint64_t handle, char* out, size_t cap, siz
   Scratch sc(c);
   char* slots = nullptr;
   uint32_t* lens = nullptr;
-  uint64_t* offs = nullptr;
+  uint32_t* bsum = nullptr;
+  uint64_t* boff = nullptr;
   uint64_t* totals = nullptr;
   int r;
   if ((r = sc.get(&slots, vtk_slot_bytes(n))) || (r = sc.get(&lens, 3 * (size_t)n)) ||
-      (r = sc.get(&offs, 3 * (size_t)n)) || (r = sc.get(&totals, 3)))
+      (r = sc.get(&bsum, 3 * vtk_blocks(n))) || (r = sc.get(&boff, 3 * vtk_blocks(n))) || (r = sc.get(&totals, 3)))
     return r;
-  launch_vtk_format(c->part + start, n, slots, lens, offs, totals, c->sms, c->stream);
+  launch_vtk_format(c->part + start, n, slots, lens, bsum, boff, totals, c->sms, c->stream);
   CK(cudaGetLastError());
   uint64_t t[3];
   CK(cudaMemcpyAsync(t, totals, sizeof t, cudaMemcpyDeviceToHost, c->stream));
@@ -974,7 +975,7 @@ int bhg_snapshot_vtk(bhg_context* c, uint64_t handle, char* out, size_t cap, siz
   char* dev = nullptr;
   if ((r = sc.get(&dev, t[0] + t[1] + t[2]))) return r;
   char* sect[3] = {dev, dev + t[0], dev + t[0] + t[1]};
-  launch_vtk_gather(slots, n, lens, offs, sect, c->sms, c->stream);
+  launch_vtk_gather(slots, n, lens, boff, sect, c->stream);
   CK(cudaGetLastError());
   const std::string* head[3] = {&h0, &h1, &h2};
   size_t at = 0;

@@ -244,33 +244,46 @@ __global__ void __launch_bounds__(128) k_vtk_format(const Particle* __restrict__
   }
 }
 
-// Copies the m slots (slot size `slot`, lengths len[], exclusive offsets
-// off[]) back to back into out, one warp per slot.
-__global__ void k_vtk_gather(const char* __restrict__ slots, int slot, const uint32_t* __restrict__ len,
-                             const uint64_t* __restrict__ off, uint64_t m, char* __restrict__ out) {
-  const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  for (uint64_t i = wid; i < m; i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
-    const uint32_t l = len[i];
-    for (uint32_t c = lane; c < l; c += 32) out[off[i] + c] = slots[i * slot + c];
-  }
+// Per-block sums of 32-bit lengths (blocks of kCsvThreads entries).
+__global__ void __launch_bounds__(kCsvThreads) k_len_sums(const uint32_t* __restrict__ len, uint64_t m,
+                                                          uint32_t* __restrict__ block_sum) {
+  __shared__ uint32_t sh[32];
+  const uint64_t i = (uint64_t)blockIdx.x * kCsvThreads + threadIdx.x;
+  uint32_t total;
+  block_excl_scan(i < m ? len[i] : 0u, sh, total);
+  if (threadIdx.x == 0) block_sum[blockIdx.x] = total;
 }
 
-// Exclusive scan of 32-bit lengths into 64-bit offsets (one block); total
+// Exclusive scan of block sums into 64-bit block offsets (one block); total
 // to *total.
-__global__ void __launch_bounds__(1024) k_scan_lengths(const uint32_t* __restrict__ len, uint64_t m,
-                                                       uint64_t* __restrict__ off, uint64_t* __restrict__ total) {
+__global__ void __launch_bounds__(1024) k_scan_sums64(const uint32_t* __restrict__ sums, uint32_t m,
+                                                      uint64_t* __restrict__ off, uint64_t* __restrict__ total) {
   __shared__ uint32_t sh[32];
   uint64_t carry = 0;
-  for (uint64_t base = 0; base < m; base += blockDim.x) {
-    const uint64_t i = base + threadIdx.x;
-    const uint32_t v = i < m ? len[i] : 0u;
+  for (uint32_t base = 0; base < m; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < m ? sums[i] : 0u;
     uint32_t tot;
     const uint32_t ex = block_excl_scan(v, sh, tot);
     if (i < m) off[i] = carry + ex;
     carry += tot;
   }
   if (threadIdx.x == 0) *total = carry;
+}
+
+// Copies slot i (slot size `slot`, length len[i]) to out at its place: the
+// block's offset plus the lengths before it in the block.
+__global__ void __launch_bounds__(kCsvThreads) k_vtk_gather(const char* __restrict__ slots, int slot,
+                                                            const uint32_t* __restrict__ len,
+                                                            const uint64_t* __restrict__ block_off, uint64_t m,
+                                                            char* __restrict__ out) {
+  __shared__ uint32_t sh[32];
+  const uint64_t i = (uint64_t)blockIdx.x * kCsvThreads + threadIdx.x;
+  const uint32_t l = i < m ? len[i] : 0u;
+  uint32_t total;
+  const uint64_t at = block_off[blockIdx.x] + block_excl_scan(l, sh, total);
+  const char* src = slots + i * slot;
+  for (uint32_t c = 0; c < l; ++c) out[at + c] = src[c];
 }
 
 // ---- launchers -----------------------------------------------------------------
@@ -311,9 +324,10 @@ void launch_csv_compact(const Particle* tmp, const uint32_t* keep, uint64_t m, u
 }
 
 size_t vtk_slot_bytes(uint32_t n) { return (size_t)n * (2 * kPosSlot + kMassSlot); }
+size_t vtk_blocks(uint32_t n) { return ((size_t)n + kCsvThreads - 1) / kCsvThreads; }
 
-void launch_vtk_format(const Particle* p, uint32_t n, char* slots, uint32_t* len, uint64_t* off, uint64_t* totals,
-                       int sms, cudaStream_t s) {
+void launch_vtk_format(const Particle* p, uint32_t n, char* slots, uint32_t* len, uint32_t* block_sum,
+                       uint64_t* block_off, uint64_t* totals, int sms, cudaStream_t s) {
   if (n == 0) return;
   unsigned blocks = (n + 127) / 128;
   if (blocks > (unsigned)sms * 16) blocks = sms * 16;
@@ -321,18 +335,22 @@ void launch_vtk_format(const Particle* p, uint32_t n, char* slots, uint32_t* len
   char* mass = slots + (size_t)n * kPosSlot;
   char* vel = mass + (size_t)n * kMassSlot;
   k_vtk_format<<<blocks, 128, 0, s>>>(p, n, pos, mass, vel, len);
-  for (int k = 0; k < 3; ++k) k_scan_lengths<<<1, 1024, 0, s>>>(len + (size_t)k * n, n, off + (size_t)k * n, totals + k);
+  const size_t nb = vtk_blocks(n);
+  for (int k = 0; k < 3; ++k) {
+    k_len_sums<<<(unsigned)nb, kCsvThreads, 0, s>>>(len + (size_t)k * n, n, block_sum + k * nb);
+    k_scan_sums64<<<1, 1024, 0, s>>>(block_sum + k * nb, (uint32_t)nb, block_off + k * nb, totals + k);
+  }
 }
 
-void launch_vtk_gather(const char* slots, uint32_t n, const uint32_t* len, const uint64_t* off, char* const out[3],
-                       int sms, cudaStream_t s) {
+void launch_vtk_gather(const char* slots, uint32_t n, const uint32_t* len, const uint64_t* block_off,
+                       char* const out[3], cudaStream_t s) {
   if (n == 0) return;
   const char* base[3] = {slots, slots + (size_t)n * kPosSlot, slots + (size_t)n * (kPosSlot + kMassSlot)};
   const int size[3] = {kPosSlot, kMassSlot, kPosSlot};
-  unsigned blocks = (n + 7) / 8;
-  if (blocks > (unsigned)sms * 32) blocks = sms * 32;
+  const size_t nb = vtk_blocks(n);
   for (int k = 0; k < 3; ++k)
-    k_vtk_gather<<<blocks, 256, 0, s>>>(base[k], size[k], len + (size_t)k * n, off + (size_t)k * n, n, out[k]);
+    k_vtk_gather<<<(unsigned)nb, kCsvThreads, 0, s>>>(base[k], size[k], len + (size_t)k * n, block_off + k * nb, n,
+                                                      out[k]);
 }
 
 }  // namespace bhg

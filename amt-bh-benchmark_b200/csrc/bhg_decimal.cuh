@@ -392,6 +392,28 @@ BHG_HD int format_g6(double x, char* out, Big& a, Big& b) {
   uint64_t D = 0;
   for (int attempt = 0; attempt < 4; ++attempt) {
     const int p = X - 5;
+    // fast path: |x| / 10^p = A / B with A = M 2^max(E,0) 10^max(-p,0) and
+    // B = 2^max(-E,0) 10^max(p,0), exact in 128 bits for moderate exponents
+    // (10^k < 2^(3.33 k): the bounds below keep A < 2^127 and B < 2^125)
+    const int e_up = E > 0 ? E : 0, e_dn = E < 0 ? -E : 0, p_up = p < 0 ? -p : 0, p_dn = p > 0 ? p : 0;
+    if (53 + e_up + (p_up * 10 + 2) / 3 <= 126 && e_dn + (p_dn * 10 + 2) / 3 <= 124) {
+      unsigned __int128 A = (unsigned __int128)M << e_up, B = (unsigned __int128)1 << e_dn;
+      for (int i = 0; i < p_up; ++i) A *= 10u;
+      for (int i = 0; i < p_dn; ++i) B *= 10u;
+      const unsigned __int128 qv = A / B, r = A - qv * B;
+      if (qv < 100000u) {
+        --X;
+        continue;
+      }
+      if (qv >= 1000000u) {
+        ++X;
+        continue;
+      }
+      D = (uint64_t)qv;
+      if (2 * r > B || (2 * r == B && (D & 1u))) ++D;
+      if (D == 1000000u) D = 100000u, ++X;
+      break;
+    }
     big_set(a, M);
     big_set(b, 1);
     if (E >= 0) big_shl(a, E);

@@ -83,10 +83,11 @@ size_t csv_keep_blocks(uint64_t m);
 void launch_csv_compact(const Particle* tmp, const uint32_t* keep, uint64_t m, uint32_t* block_count,
                         uint64_t* total, Particle* dst, cudaStream_t s);
 size_t vtk_slot_bytes(uint32_t n);
-void launch_vtk_format(const Particle* p, uint32_t n, char* slots, uint32_t* len, uint64_t* off, uint64_t* totals,
-                       int sms, cudaStream_t s);
-void launch_vtk_gather(const char* slots, uint32_t n, const uint32_t* len, const uint64_t* off, char* const out[3],
-                       int sms, cudaStream_t s);
+size_t vtk_blocks(uint32_t n);
+void launch_vtk_format(const Particle* p, uint32_t n, char* slots, uint32_t* len, uint32_t* block_sum,
+                       uint64_t* block_off, uint64_t* totals, int sms, cudaStream_t s);
+void launch_vtk_gather(const char* slots, uint32_t n, const uint32_t* len, const uint64_t* block_off,
+                       char* const out[3], cudaStream_t s);
 
 // n particles of one Plummer sphere (scale a, total mass `mass`, centre c[3],
 // bulk velocity b[3], ids id0..), drawn from a counter-based generator keyed

@@ -621,6 +621,14 @@ def bench_csv(args, w, rig, bhg, peaks):
         ems, _, _ = rig.time_steps(e2e_step, args.steps, 1)
         out["e2e"] = {"value": ps / (ems / 1000.0), "unit": "particles/s", "h2d_bytes_per_step": nb,
                       "d2h_bytes_per_step": 0, "path": "bhg_upload_csv from pinned host memory"}
+    # write_vtk on the device: formatted there, the text copied back
+    snap = ctx.snapshot_vtk()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        snap = ctx.snapshot_vtk()
+    snap_s = (time.perf_counter() - t0) / 3
+    out["snapshot_vtk"] = {"particles_per_s": n / snap_s, "ms": snap_s * 1000.0, "bytes": len(snap),
+                           "path": "bhg_snapshot_vtk into host memory (wall clock)"}
     ctx.close()
     if rig.rank == 0 and not args.no_cpu_baseline:
         try:
@@ -628,6 +636,10 @@ def bench_csv(args, w, rig, bhg, peaks):
             from oracle import Reference
 
             ref = Reference()
+            t0 = time.perf_counter()
+            ref_snap = ref.write_vtk(parts)
+            out["snapshot_vtk"]["reference_particles_per_s"] = n / (time.perf_counter() - t0)
+            out["snapshot_vtk"]["same_bytes_as_reference"] = ref_snap == snap
             with tempfile.NamedTemporaryFile(suffix=".csv", delete=False) as f:
                 f.write(text)
                 path = f.name
