@@ -117,7 +117,14 @@ struct SplitEval {
   float4* stage;  // records: cells 3 float4 each, particles 1 float4 each
   double* red;    // per-lane FP64 sums at the end of a walk (aliases stage)
   double cx, cy, cz;  // reference point: the walk box's centre
-  float eps2;
+  float eps2;         // softening in scaled units
+  // the FP32 arithmetic runs on offsets times a power of two near the
+  // system's size (1 / 2^ilogb(domain half width)), so that r^-7 of the
+  // smallest and largest systems stays inside FP32's range; the powers of two
+  // make the scaling exact (rsqrt of an even power of two too), and the FP64
+  // sums are scaled back
+  double scale = 1.0, unscale2 = 1.0;  // see set_system
+  float scale2f = 1.f;
   int lane, tb, kt, lpg, ng, first, stride, offb;
   float t0x, t0y, t0z, t1x, t1y, t1z;  // target positions (t1 = t0 when kt = 1)
   float a0x, a0y, a0z, a1x, a1y, a1z;  // FP32 partials of the current batch
@@ -136,6 +143,16 @@ struct SplitEval {
 
   __device__ int cell_chunk() const { return kCellBatch; }
   __device__ int part_chunk() const { return kPartBatch; }
+
+  // softening eps2_ and the system's domain half width hw
+  __device__ void set_system(double eps2_, double hw) {
+    int k = hw > 0.0 ? ilogb(hw) : 0;
+    k = k < -100 ? -100 : (k > 100 ? 100 : k);
+    scale = ldexp(1.0, -k);            // offsets d' = d * scale
+    unscale2 = ldexp(1.0, -2 * k);     // a = a' * scale^2 (a' = m d' / r'^3 = a / scale^2)
+    scale2f = (float)ldexp(1.0, -2 * k);  // Q' = Q * scale^2, eps2' = eps2 * scale^2
+    eps2 = (float)(eps2_ * (scale * scale));
+  }
 
   // targets: particles p0 .. p0 + n - 1 (n <= 64); their FP64 sums are
   // added to sums[0 .. n)
@@ -156,18 +173,20 @@ struct SplitEval {
     offb = kt == 1 ? ng : 0;
     const int t0 = slot, t1 = (kt == 2 && slot + lpg < tb) ? slot + lpg : slot;
     const double4 q0 = a.pm[p0 + t0], q1 = a.pm[p0 + t1];
-    t0x = (float)__dsub_rn(q0.x, cx), t0y = (float)__dsub_rn(q0.y, cy), t0z = (float)__dsub_rn(q0.z, cz);
-    t1x = (float)__dsub_rn(q1.x, cx), t1y = (float)__dsub_rn(q1.y, cy), t1z = (float)__dsub_rn(q1.z, cz);
+    t0x = (float)(__dsub_rn(q0.x, cx) * scale), t0y = (float)(__dsub_rn(q0.y, cy) * scale);
+    t0z = (float)(__dsub_rn(q0.z, cz) * scale);
+    t1x = (float)(__dsub_rn(q1.x, cx) * scale), t1y = (float)(__dsub_rn(q1.y, cy) * scale);
+    t1z = (float)(__dsub_rn(q1.z, cz) * scale);
     a0x = a0y = a0z = a1x = a1y = a1z = 0.f;
     s0x = s0y = s0z = s1x = s1y = s1z = 0.0;
   }
 
   __device__ __forceinline__ void flush() {
-    s0x += (double)a0x, s0y += (double)a0y, s0z += (double)a0z;
+    s0x += (double)a0x * unscale2, s0y += (double)a0y * unscale2, s0z += (double)a0z * unscale2;
     if (kt == 1) {
-      s0x += (double)a1x, s0y += (double)a1y, s0z += (double)a1z;
+      s0x += (double)a1x * unscale2, s0y += (double)a1y * unscale2, s0z += (double)a1z * unscale2;
     } else {
-      s1x += (double)a1x, s1y += (double)a1y, s1z += (double)a1z;
+      s1x += (double)a1x * unscale2, s1y += (double)a1y * unscale2, s1z += (double)a1z * unscale2;
     }
     a0x = a0y = a0z = a1x = a1y = a1z = 0.f;
   }
@@ -219,15 +238,15 @@ struct SplitEval {
       const WNode* w = a.w + n;
       const double2 cxy = *reinterpret_cast<const double2*>(&w->cx);
       const double czz = w->cz;
-      const float4 r0 = make_float4((float)__dsub_rn(cxy.x, cx), (float)__dsub_rn(cxy.y, cy),
-                                    (float)__dsub_rn(czz, cz), w->mass);
+      const float4 r0 = make_float4((float)(__dsub_rn(cxy.x, cx) * scale), (float)(__dsub_rn(cxy.y, cy) * scale),
+                                    (float)(__dsub_rn(czz, cz) * scale), w->mass);
       stage[3 * i] = r0;
       if (QUAD) {
         const float4 qa = *reinterpret_cast<const float4*>(w->q);
         const float2 qb = a.q45[n];
-        // record layout: (q0 q1 q2 q3) (q4 q5 - -)
-        stage[3 * i + 1] = qa;
-        stage[3 * i + 2] = make_float4(qb.x, qb.y, 0.f, 0.f);
+        // record layout: (q0 q1 q2 q3) (q4 q5 - -), in scaled units
+        stage[3 * i + 1] = make_float4(qa.x * scale2f, qa.y * scale2f, qa.z * scale2f, qa.w * scale2f);
+        stage[3 * i + 2] = make_float4(qb.x * scale2f, qb.y * scale2f, 0.f, 0.f);
       }
     }
     __syncwarp();
@@ -244,8 +263,8 @@ struct SplitEval {
   __device__ void parts(const uint32_t* ring, uint32_t head, int cnt) {
     for (int i = lane; i < cnt; i += 32) {
       const double4 p = a.pm[ring[(head + (uint32_t)i) & (kPartQ - 1)]];
-      stage[i] = make_float4((float)__dsub_rn(p.x, cx), (float)__dsub_rn(p.y, cy), (float)__dsub_rn(p.z, cz),
-                             (float)p.w);
+      stage[i] = make_float4((float)(__dsub_rn(p.x, cx) * scale), (float)(__dsub_rn(p.y, cy) * scale),
+                             (float)(__dsub_rn(p.z, cz) * scale), (float)p.w);
     }
     if (lane == 0) stage[kPartDummy] = make_float4(kFarAway, 0.f, 0.f, 0.f);
     __syncwarp();
@@ -298,6 +317,7 @@ struct F64Eval {
 
   __device__ int cell_chunk() const { return 2 * L; }
   __device__ int part_chunk() const { return 2 * L; }
+  __device__ void set_system(double eps2_, double) { eps2 = eps2_; }
 
   static __device__ int groups_for(int tb) {
     return tb <= 2 ? 1 : tb <= 4 ? 2 : tb <= 8 ? 4 : tb <= 16 ? 8 : tb <= 32 ? 16 : 32;
@@ -689,7 +709,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     const uint32_t root = a.sys[s].root;
     const SysParam& sp = a.prm[s];
     const double theta2 = sp.theta2;
-    ev.eps2 = sp.eps2;
+    ev.set_system(sp.eps2, a.sys[s].hw);
     uint32_t ti = a.group_first[gi];
     const bool single = ti < ntargets && a.targets[ti] == gnode;  // the group is its own target
     bool group_job = !single, shared = false;
