@@ -287,13 +287,46 @@ def cpu_serve_sample(w, budget_particles=600000):
     return n_tot / t_tot, threads, sample
 
 
+def cpu_csv_sample(w):
+    """The reference's read_csv (mmap + one thread per usable CPU) on the
+    workload's CSV text, after one untimed read: (particles/s, threads, sample)."""
+    import ctypes
+
+    import bhg
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference
+
+    parts, _ = bhg.plummer(w["n"], w["seed"])
+    ref = Reference()
+    with tempfile.NamedTemporaryFile(suffix=".csv", delete=False) as f:
+        path = f.name
+    try:
+        bhg.write_csv(path, parts)
+        buf = np.zeros(w["n"] + 1, bhg.PARTICLE)
+        cnt = ctypes.c_size_t()
+        err = ctypes.create_string_buffer(256)
+        ref.lib.bhref_read_csv(path.encode(), buf.ctypes.data, len(buf), ctypes.byref(cnt), err, 256)
+        t0 = time.perf_counter()
+        ref.lib.bhref_read_csv(path.encode(), buf.ctypes.data, len(buf), ctypes.byref(cnt), err, 256)
+        dt = time.perf_counter() - t0
+        nb = os.path.getsize(path)
+    finally:
+        os.unlink(path)
+    return w["n"] / dt, os.cpu_count(), f"the full text ({nb} bytes) through read_csv, after one untimed read"
+
+
 def reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import bhg
 
-    if w["kind"] == "serve":
+    unit = "particle-steps/s" if w["kind"] != "csv" else "particles/s"
+    if w["kind"] == "csv":
+        value, threads, sample = cpu_csv_sample(w)
+        ms_step = w["n"] / value * 1000.0
+    elif w["kind"] == "serve":
         value, threads, sample = cpu_serve_sample(w)
         ms_step = None
     elif w["kind"] == "ensemble":
@@ -312,13 +345,14 @@ def reference_arm(args, w):
                   f"{len(timed)} force evaluations of the reference schedule through bh::step_particles, "
                   f"rate = N*{w['steps']}/({w['steps'] + 1}*mean eval time)")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC if w["kind"] != "csv" else "csv-ingest particles/s", "value": value,
+        "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, **{k: v for k, v in w.items() if k != "kind"}, "threads": threads},
-        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "reference",
                          "sample": sample},
-        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
