@@ -85,3 +85,15 @@ def test_empty_and_header_only_texts(gpu):
         with pytest.raises(bhg.BhgError) as e:
             gpu.upload_csv(text)
         assert "no particles" in str(e.value)
+
+
+@pytest.mark.parametrize("name", ["text_mixed", "text_crlf"])
+def test_gpu_matches_text_golden(gpu, name):
+    """The reference's own read_csv/write_vtk outputs, committed, against the GPU."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+    gpu.upload_csv(g["text"].tobytes())
+    got = gpu.download()
+    assert same(got, g["particles"])
+    assert gpu.snapshot_vtk() == g["vtk"].tobytes()

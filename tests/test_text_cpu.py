@@ -78,3 +78,13 @@ def test_decimal_conversions_match_the_cxx_library(tmp_path):
     out = subprocess.run([str(exe), "100000"], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.startswith("ok")
+
+
+@pytest.mark.parametrize("name", ["text_mixed", "text_crlf"])
+def test_oracle_matches_text_golden(oracle, name):
+    """The reference's own read_csv/write_vtk outputs, committed (made by
+    tests/golden/make_text_golden.py), against the oracle, anywhere."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", name + ".npz"))
+    got, bad = oracle.read_csv(g["text"].tobytes())
+    assert bad is None and same(got, g["particles"])
+    assert oracle.write_vtk(g["particles"]) == g["vtk"].tobytes()
