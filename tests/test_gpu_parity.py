@@ -91,6 +91,47 @@ def test_theta0_is_direct_sum(gpu, oracle, precision, tol):
     assert rel_error(acc, ref) <= tol
 
 
+@pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-12), (bhg.PRECISION_SPLIT, 1e-6)])
+@pytest.mark.parametrize("max_leaf,theta", [(4, 0.5), (1, 0.7)], ids=["pair", "cell"])
+def test_two_body_analytic(gpu, precision, tol, max_leaf, theta):
+    """test_force_kernel.cc:17-43 through the whole GPU path: a source of mass
+    3 at distance 4 pulls with G m / 16 (G = 2), whether it arrives as a direct
+    particle (one leaf) or as an accepted one-particle cell whose second moment
+    is zero; softening weakens it."""
+    parts = np.zeros(2, dtype=bhg.PARTICLE)
+    parts["id"] = [0, 1]
+    parts["mass"] = [1.0, 3.0]
+    parts["pos"][1] = (4.0, 0.0, 0.0)
+    for eps2, mag in ((0.0, 2.0 / 16.0), (4.0, 2.0 * 4.0 / 20.0 ** 1.5)):
+        gpu.upload(parts)
+        gpu.build_tree(max_leaf, 16)
+        gpu.compute_multipoles()
+        acc = gpu.walk_forces(bhg.Context.params(theta, eps2, 2.0, True, precision), 0)
+        out = gpu.download()
+        a0 = acc[out["id"] == 0][0]
+        a1 = acc[out["id"] == 1][0]
+        assert abs(a0[0] - 3.0 * mag) <= tol * 3.0 * mag and abs(a0[1]) + abs(a0[2]) <= tol * mag
+        assert abs(a1[0] + mag) <= tol * mag and abs(a1[1]) + abs(a1[2]) <= tol * mag
+
+
+@pytest.mark.parametrize("precision", [bhg.PRECISION_FP64, bhg.PRECISION_SPLIT])
+def test_quadrupole_beats_monopole(gpu, oracle, precision):
+    """test_bh_vs_bruteforce.cc:78-113: two tight clusters 100 apart, theta
+    0.6, leaf 4: the quadrupole term lowers the error against the direct sum."""
+    parts = np.concatenate([cube(100, 2, spread=1.0, centre=(-50.0, 0.0, 0.0)),
+                            cube(100, 3, spread=1.0, centre=(50.0, 0.0, 0.0))])
+    parts["id"] = np.arange(200)
+    err = {}
+    for quad in (False, True):
+        gpu.upload(parts)
+        gpu.build_tree(4, 64)
+        gpu.compute_multipoles()
+        acc = gpu.walk_forces(bhg.Context.params(0.6, 1e-6, 1.0, quad, precision), 0)
+        out = gpu.download()
+        err[quad] = rel_error(acc, oracle.direct(soa(out), np.arange(len(out)), 1e-6))
+    assert err[True] < err[False], err
+
+
 def test_no_softening_masks_self(gpu, oracle):
     # eps = 0: r^2 == 0 entries masked (accumulate_list Mask, grouped_ttg.h:117-123)
     parts = cube(3000, 9)
