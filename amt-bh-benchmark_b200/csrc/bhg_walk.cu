@@ -29,7 +29,7 @@
 //
 // Split precision: sources and targets become FP32 offsets from the walk's
 // bounding-box centre (the subtraction in FP64), staged once per batch in
-// shared memory; interactions are FP32 FMA + rsqrtf with lanes laid out as
+// shared memory; interactions are FP32 FMA + rsqrt.approx.ftz, lanes laid out as
 // (target, source subset) (SplitEval below); FP32 partials go into FP64
 // sums after every batch.  The kick/drift of integrate_ttg.h:74-77 is
 // applied in FP64 in the epilogue.
@@ -108,6 +108,16 @@ __device__ __forceinline__ double far2(const double lo[3], const double hi[3], d
 // (kt = 2).  FP32 partials are added into per-lane FP64 sums after every
 // batch; at the end of a walk the lane groups' FP64 sums are added in group
 // order (deterministic) into the targets' FP64 sums.
+// rsqrt.approx.ftz.f32 (PTX ISA): the approximate reciprocal square root,
+// subnormal inputs and results flushed to zero.  The split evaluator's r^2 is
+// in units scaled to the system's size (at least eps^2 there, or masked when
+// eps = 0), so the flush only drops contributions below FP32's normal range.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 template <bool QUAD, bool MASK>
 struct SplitEval {
   static constexpr int kCellBatch = 64, kPartBatch = 128;
@@ -197,7 +207,7 @@ struct SplitEval {
     const float4 r0 = r[0];
     const float dx = r0.x - tx, dy = r0.y - ty, dz = r0.z - tz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-    float ri = rsqrtf(r2);
+    float ri = rsqrt_ftz(r2);
     if (!QUAD && MASK) ri = r2 > 0.f ? ri : 0.f;
     const float ri2 = ri * ri;
     const float ri3 = ri * ri2;
@@ -212,9 +222,9 @@ struct SplitEval {
       const float ri5 = ri3 * ri2;
       // m d / r^3 - Q d / r^5 + 2.5 (d Q d) d / r^7
       const float c = fmaf(2.5f * dqd, ri5 * ri2, r0.w * ri3);
-      ax += fmaf(c, dx, -ri5 * qx);
-      ay += fmaf(c, dy, -ri5 * qy);
-      az += fmaf(c, dz, -ri5 * qz);
+      ax = fmaf(-ri5, qx, fmaf(c, dx, ax));
+      ay = fmaf(-ri5, qy, fmaf(c, dy, ay));
+      az = fmaf(-ri5, qz, fmaf(c, dz, az));
     } else {
       const float c = r0.w * ri3;
       ax = fmaf(c, dx, ax), ay = fmaf(c, dy, ay), az = fmaf(c, dz, az);
@@ -225,7 +235,7 @@ struct SplitEval {
                                             float& az) const {
     const float dx = r.x - tx, dy = r.y - ty, dz = r.z - tz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-    float ri = rsqrtf(r2);
+    float ri = rsqrt_ftz(r2);
     if (MASK) ri = r2 > 0.f ? ri : 0.f;
     const float c = r.w * (ri * ri) * ri;
     ax = fmaf(c, dx, ax), ay = fmaf(c, dy, ay), az = fmaf(c, dz, az);
