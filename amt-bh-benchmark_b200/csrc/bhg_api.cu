@@ -17,7 +17,6 @@ using namespace bhg;
 
 namespace {
 
-
 // Phases of one evaluation, each timed with CUDA events and, in bhg_step,
 // replayed from its own captured graph.
 enum Phase { kPre, kSort, kTree, kMoments, kTargets, kWalk, kPhases };
@@ -42,10 +41,14 @@ struct bhg_context {
   std::vector<Tile> tiles_host;
   std::vector<std::pair<void*, size_t>> allocs;
 
-  // capacities
   // capacities (cap_n covers the scratch, cap_part the state; a capacity is
   // 0 after a growth that failed part-way)
-  size_t cap_n = 0, cap_part = 0, cap_nodes = 0, cap_sys = 0, cap_tiles = 0, cap_stack_warps = 0;
+  size_t cap_n = 0, cap_part = 0, cap_nodes = 0, cap_sys = 0, cap_tiles = 0;
+  // the walk's two-pass schedule: buffers for split_cap groups (0: one pass
+  // only; split_failed: the budget had no room, not tried again)
+  void* split_buf = nullptr;
+  size_t split_cap = 0;
+  bool split_failed = false;
 
   // device buffers
   Particle *part = nullptr, *staged = nullptr;
@@ -252,11 +255,31 @@ int walk_grid(bhg_context* c) {
   return c->sms * per;
 }
 
-int ensure_stack(bhg_context* c, int grid) {
-  // the walk keeps its stacks in shared memory; this only makes sure the
-  // kernel's occupancy (and shared-memory limit) is set up before capture
-  size_t warps = (size_t)grid * (walk_threads() / 32);
-  c->cap_stack_warps = std::max(c->cap_stack_warps, warps);
+// Walk groups per resident warp up to which the walk runs its two-pass
+// schedule (k_walk: group walks, then every target walk as a job of its
+// own).  Measured on Plummer spheres: the two passes take 25% less time at
+// 65k particles, 19% at 131k, 10% at 262k, 1% at 524k (37k groups is about
+// 16 per warp) and never more; past that the groups alone keep every warp
+// busy.  The buffers take 3.5 KB per group (136 MB with 2,368 warps).
+constexpr size_t kSplitGroupsPerWarp = 16;
+
+// The buffers of the walk's two-pass schedule, allocated before the walk is
+// captured (walk_grid has also set the kernels' shared-memory limit by
+// then).  Without room for them in the HBM budget the walk keeps the
+// one-pass schedule, which gives the same bits.
+int ensure_walk_scratch(bhg_context* c, int grid) {
+  const size_t groups = (size_t)grid * (walk_threads() / 32) * kSplitGroupsPerWarp;
+  if (c->split_cap >= groups || c->split_failed) return BHG_OK;
+  drop_graph(c);
+  dev_free(c, c->split_buf);
+  c->split_buf = nullptr;
+  c->split_cap = 0;
+  if (dev_alloc(c, &c->split_buf, groups * walk_split_bytes_per_group()) != BHG_OK) {
+    c->err.clear();
+    c->split_failed = true;
+    return BHG_OK;
+  }
+  c->split_cap = groups;
   return BHG_OK;
 }
 
@@ -386,6 +409,10 @@ void enq_walk(bhg_context* c, bool want_accel) {
   a.out = c->part;
   a.accel = want_accel ? c->accel : nullptr;
   a.st = c->st;
+  a.gsum = static_cast<double*>(c->split_buf);
+  a.gdefer = reinterpret_cast<uint32_t*>(a.gsum + c->split_cap * kGroupMax * 3);
+  a.gnd = a.gdefer + c->split_cap * walk_defer_cap();
+  a.split_max = (uint32_t)c->split_cap;
   launch_walk(a, c->precision, c->quad != 0, c->mask, walk_grid(c), c->stream);
   launch_eval_done(c->st, c->stream);
 }
@@ -474,7 +501,7 @@ int run_phase(bhg_context* c, int phase, bool graphed, const std::string& key, F
 
 std::string graph_key(const bhg_context* c, uint32_t target_size) {
   char key[192];
-  snprintf(key, sizeof key, "%zu/%d/%zu/%zu/%u/%u/%u/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->cap_stack_warps,
+  snprintf(key, sizeof key, "%zu/%d/%zu/%zu/%u/%u/%u/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->split_cap,
            c->max_leaf, c->group_size, target_size, c->precision, c->quad, (int)c->mask);
   return key;
 }
@@ -1042,7 +1069,7 @@ int bhg_walk_forces(bhg_context* c, const bhg_force_params* fp, uint32_t target_
   int r = set_force_params(c, fp, kick_dt, drift_dt, false);
   if (r) return r;
   if (!c->accel && (r = grow(c, &c->accel, c->cap_n * 3))) return r;
-  if ((r = ensure_stack(c, walk_grid(c))) || (r = push_params(c))) return r;
+  if ((r = ensure_walk_scratch(c, walk_grid(c))) || (r = push_params(c))) return r;
   if ((r = run_phase(c, kTargets, false, "", [&] { enq_targets(c, target_size); })) ||
       (r = run_phase(c, kWalk, false, "", [&] { enq_walk(c, true); })))
     return r;
@@ -1116,7 +1143,7 @@ int prepare_step(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, 
   if (c->max_leaf != max_leaf || c->group_size != group_size) drop_graph(c);
   c->max_leaf = max_leaf;
   c->group_size = group_size;
-  if ((r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf))) || (r = ensure_stack(c, walk_grid(c))))
+  if ((r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf))) || (r = ensure_walk_scratch(c, walk_grid(c))))
     return r;
   return BHG_OK;
 }
@@ -1149,7 +1176,7 @@ int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<
     if (c->st_host->status & kStNodeOverflow) {
       next += done;
       size_t need = std::max<size_t>(2 * c->cap_nodes, (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64);
-      if ((r = clear_status(c)) || (r = ensure_nodes(c, need)) || (r = ensure_stack(c, walk_grid(c)))) return r;
+      if ((r = clear_status(c)) || (r = ensure_nodes(c, need)) || (r = ensure_walk_scratch(c, walk_grid(c)))) return r;
       continue;
     }
     r = check_status(c);
@@ -1217,7 +1244,7 @@ int bhg_get_stats(bhg_context* c, bhg_stats* out, int reset) {
   // one per level; one multipole kernel per level; mark + compact of the
   // targets and of the groups + first target per group; walk + its
   // completion count
-  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (kMortonDepth + 1) + 5 + 2;
+  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (kMortonDepth + 1) + 5 + 2 + (c->split_cap ? 1 : 0);
   if (reset) {
     for (double& t : c->tot_ms) t = 0.0;
     c->walks_timed = 0;

@@ -99,7 +99,7 @@ struct DevState {
   uint32_t walk_next;        // next group of the walk
   uint32_t scan_tiles;       // tiles taken by the target compaction
   uint32_t group_tiles;      // tiles taken by the group compaction
-  uint32_t pad0;
+  uint32_t walk_next2;       // next target of the walk's second pass
   unsigned long long pp, pc;  // interaction counts of the walk
 };
 constexpr size_t kBuildResetOffset = offsetof(DevState, n_nodes);

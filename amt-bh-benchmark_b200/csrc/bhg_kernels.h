@@ -51,6 +51,12 @@ struct WalkArgs {
   Particle* out;           // kicked/drifted particles (the state)
   double* accel;           // optional: G*a, 3 per particle
   DevState* st;
+  // the two-pass schedule for few walk groups (k_walk): groups' shared
+  // parts (kGroupMax x 3 per group), deferred nodes, deferred counts
+  double* gsum;
+  uint32_t* gdefer;
+  uint32_t* gnd;
+  uint32_t split_max;  // two passes when n_groups <= split_max (0: never)
 };
 
 // Walks every target and kicks/drifts its particles.  precision:
@@ -58,6 +64,9 @@ struct WalkArgs {
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s);
 int walk_blocks_per_sm(int precision, bool quad, bool mask);
 int walk_threads();
+// device bytes per group of the two-pass schedule's buffers; deferred slots per group
+size_t walk_split_bytes_per_group();
+size_t walk_defer_cap();
 
 void launch_integrate(Particle* p, const double* accel, uint32_t n, const SysDev* sys, const SysParam* prm, int nsys,
                       int sms, cudaStream_t s);

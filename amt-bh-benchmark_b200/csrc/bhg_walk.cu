@@ -687,9 +687,31 @@ __device__ __forceinline__ void kick_drift(const WalkArgs& a, const SysParam& sp
   __syncwarp();
 }
 
+// The system holding particle p (systems lie back to back).
+__device__ __forceinline__ uint32_t system_of(const WalkArgs& a, uint32_t p) {
+  uint32_t lo = 0, hi = (uint32_t)a.nsys;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a.sys[mid].begin <= p) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+constexpr uint32_t kNotShared = 0xffffffffu;  // the group walk gave up: targets walk from the root
+
 // One warp per walk group.  The walks of a group - its shared group walk,
 // then one per target (one per kGroupMax particles of a large leaf target) -
 // run as consecutive jobs through a single walk_and_sum call.
+//
+// With few groups (n_groups <= a.split_max: about as many groups as warps,
+// so the largest group would set the kernel's time) the work is cut in two
+// passes instead: this kernel runs the group walks (and the groups that are
+// their own target) and leaves each group's shared part and deferred nodes
+// in a.gsum / a.gdefer / a.gnd; k_walk_targets then runs every target walk
+// as a job of its own.  Both schedules run the same walks and add the
+// target's part onto the group's part the same way, so the results are the
+// same bits.
 template <class E, bool QUAD>
 __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -697,6 +719,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
   if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;  // the build failed: touch nothing
   const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
+  const bool two_pass = ngroups <= a.split_max;
   unsigned long long n_pp = 0, n_pc = 0;
   E ev(a, S.stage, lane);
   for (;;) {
@@ -706,16 +729,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     if (gi >= ngroups) break;
     const uint32_t gnode = a.groups[gi];
     const uint32_t gb = a.nbegin[gnode], gn = a.ncount[gnode];
-    uint32_t s = 0;
-    if (a.nsys > 1) {  // the system holding particle gb
-      uint32_t lo = 0, hi = (uint32_t)a.nsys;
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (a.sys[mid].begin <= gb) lo = mid;
-        else hi = mid;
-      }
-      s = lo;
-    }
+    const uint32_t s = a.nsys > 1 ? system_of(a, gb) : 0u;
     const uint32_t root = a.sys[s].root;
     const SysParam& sp = a.prm[s];
     const double theta2 = sp.theta2;
@@ -756,6 +770,15 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
           for (uint32_t i = lane; i < gn; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
           __syncwarp();
         }
+        if (two_pass) {  // the targets walk in k_walk_targets
+          double* g = a.gsum + (size_t)gi * (kGroupMax * 3);
+          for (uint32_t i = lane; i < gn; i += 32) g[3 * i] = S.acc[i][0], g[3 * i + 1] = S.acc[i][1], g[3 * i + 2] = S.acc[i][2];
+          if (shared)
+            for (uint32_t i = lane; i < ndefer; i += 32) a.gdefer[(size_t)gi * kDeferCap + i] = S.defer[i];
+          if (lane == 0) a.gnd[gi] = shared ? ndefer : kNotShared;
+          __syncwarp();
+          break;
+        }
         continue;
       }
       if (single) {  // a batch of a large target is written out right away
@@ -771,7 +794,70 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
       __syncwarp();
       ++ti;
     }
-    if (!single) kick_drift(a, sp, S.acc, gb, gn, lane);
+    if (!single && !two_pass) kick_drift(a, sp, S.acc, gb, gn, lane);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.st->pp, n_pp);
+    atomicAdd(&a.st->pc, n_pc);
+  }
+}
+
+// The second pass of the two-pass schedule (see k_walk): one warp per target
+// of a group that is not its own target, walking from the group's deferred
+// nodes; the target's part goes onto the group's shared part, then kick/drift.
+template <class E, bool QUAD>
+__global__ void __launch_bounds__(kWalkThreads, 4) k_walk_targets(WalkArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+  if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;
+  const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
+  if (ngroups > a.split_max) return;  // k_walk ran the one-pass schedule
+  unsigned long long n_pp = 0, n_pc = 0;
+  E ev(a, S.stage, lane);
+  for (;;) {
+    uint32_t ti = 0;
+    if (lane == 0) ti = atomicAdd(&a.st->walk_next2, 1u);
+    ti = __shfl_sync(kFull, ti, 0);
+    if (ti >= ntargets) break;
+    // its group: the last one whose first target is at or before ti
+    uint32_t gi = 0, hi = ngroups;
+    while (hi - gi > 1) {
+      const uint32_t mid = (gi + hi) >> 1;
+      if (a.group_first[mid] <= ti) gi = mid;
+      else hi = mid;
+    }
+    const uint32_t gnode = a.groups[gi];
+    if (a.targets[a.group_first[gi]] == gnode) continue;  // its own target: done in the first pass
+    const uint32_t tnode = a.targets[ti];
+    const uint32_t tb = a.nbegin[tnode], T = a.ncount[tnode];  // T <= kGroupMax: inside a group
+    const uint32_t gb = a.nbegin[gnode];
+    const uint32_t s = a.nsys > 1 ? system_of(a, tb) : 0u;
+    const SysParam& sp = a.prm[s];
+    const uint32_t nd = a.gnd[gi];
+    const bool shared = nd != kNotShared;
+    const double* g = a.gsum + (size_t)gi * (kGroupMax * 3) + 3 * (size_t)(tb - gb);
+    if (shared && nd == 0) {  // nothing deferred: the group's part is the whole sum
+      for (uint32_t i = lane; i < T; i += 32) S.tacc[i][0] = g[3 * i], S.tacc[i][1] = g[3 * i + 1], S.tacc[i][2] = g[3 * i + 2];
+    } else {
+      if (shared)
+        for (uint32_t i = lane; i < nd; i += 32) S.defer[i] = a.gdefer[(size_t)gi * kDeferCap + i];
+      __syncwarp();
+      ev.set_system(sp.eps2, a.sys[s].hw);
+      double lo[3], hi3[3];
+      particle_box(a.pm, tb, T, lane, lo, hi3);
+      ev.cx = 0.5 * (lo[0] + hi3[0]), ev.cy = 0.5 * (lo[1] + hi3[1]), ev.cz = 0.5 * (lo[2] + hi3[2]);
+      uint32_t nd2 = 0;
+      walk_and_sum(ev, a, S, S.tacc, a.sys[s].root, shared ? nd : 0u, lo, hi3, sp.theta2, false, tb, (int)T, lane, n_pp,
+                   n_pc, QUAD, nd2);
+      for (uint32_t i = lane; i < T; i += 32) {  // the target's own part onto the group's shared part
+        S.tacc[i][0] = g[3 * i] + S.tacc[i][0];
+        S.tacc[i][1] = g[3 * i + 1] + S.tacc[i][1];
+        S.tacc[i][2] = g[3 * i + 2] + S.tacc[i][2];
+      }
+    }
+    __syncwarp();
+    kick_drift(a, sp, S.tacc, tb, T, lane);
   }
   if (lane == 0) {
     atomicAdd(&a.st->pp, n_pp);
@@ -782,6 +868,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
 template <class E, bool QUAD>
 static void launch_one(const WalkArgs& a, int grid, cudaStream_t s) {
   k_walk<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
+  if (a.split_max) k_walk_targets<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
 }
 
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s) {
@@ -797,6 +884,7 @@ void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int gri
 template <class E, bool QUAD>
 static int occ() {
   cudaFuncSetAttribute(k_walk<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
+  cudaFuncSetAttribute(k_walk_targets<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
   int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<E, QUAD>, kWalkThreads, kWalkSmem);
   return b > 0 ? b : 1;
@@ -821,6 +909,9 @@ int walk_blocks_per_sm(int precision, bool quad, bool mask) {
 }
 
 int walk_threads() { return kWalkThreads; }
+
+size_t walk_split_bytes_per_group() { return kGroupMax * 3 * sizeof(double) + kDeferCap * sizeof(uint32_t) + sizeof(uint32_t); }
+size_t walk_defer_cap() { return kDeferCap; }
 
 // ---------------------------------------------------------------------------
 // Unfused integrate phase: kick_one / drift_one (integrate.h:15-16) with

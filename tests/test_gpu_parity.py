@@ -265,6 +265,26 @@ def test_system_alone_equals_in_the_mix(precision):
             at += len(s)
 
 
+@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
+def test_two_pass_walk_equals_one_pass(precision):
+    """With few walk groups the walk runs group walks first and every target
+    walk as a job of its own (two kernels); without room for that schedule's
+    buffers (a tight HBM budget) it runs one warp per group.  Same bits."""
+    parts = bhg.plummer(30000, 31)[0]
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, precision)
+    out, stats = {}, {}
+    for budget in (0, 14 << 20):
+        with bhg.Context(device=0, hbm_budget=budget) as ctx:
+            ctx.upload(parts)
+            for _ in range(2):
+                ctx.step(fp, 16, 256, 16, 0.01, 0.01)
+            out[budget] = ctx.download()
+            stats[budget] = ctx.stats()
+    assert stats[0]["kernels_per_eval"] == stats[14 << 20]["kernels_per_eval"] + 1  # the two schedules ran
+    assert (stats[0]["pp"], stats[0]["pc"]) == (stats[14 << 20]["pp"], stats[14 << 20]["pc"])
+    assert out[0].tobytes() == out[14 << 20].tobytes()
+
+
 @pytest.mark.parametrize("precision", [bhg.PRECISION_FP64, bhg.PRECISION_SPLIT])
 def test_energy_conservation_cold_cube(precision):
     """The scenario of the reference's test_energy_conservation.cc:13-71: a
