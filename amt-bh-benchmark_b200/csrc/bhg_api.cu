@@ -150,7 +150,7 @@ void drop_graph(bhg_context* c) {
 
 // Device bytes of one node slot (the SoA arrays, the walk record, the cut
 // lists) and of the slots one particle brings at max_leaf 16 (0.45 each).
-constexpr size_t kNodeBytes = 16 + 32 + 32 + 48 + 64 + 8 + 48 + 12 + 4;
+constexpr size_t kNodeBytes = 16 + 32 + 32 + 48 + 64 + 8 + 48 + 8 + 12 + 4;
 constexpr size_t kNodeBytesPerParticle = kNodeBytes * 45 / 100;
 // Device bytes of the particle-sized buffers, per particle: the state and
 // its staging copy, sources, sort keys and values, marks, accelerations.
@@ -177,7 +177,8 @@ int ensure_nodes(bhg_context* c, size_t need) {
   if ((r = grow(c, &c->nd.begin, cap)) || (r = grow(c, &c->nd.count, cap)) || (r = grow(c, &c->nd.first, cap)) ||
       (r = grow(c, &c->nd.info, cap)) || (r = grow(c, &c->nd.box, cap)) || (r = grow(c, &c->nd.mom, cap)) ||
       (r = grow(c, &c->nd.iab, cap * 6)) || (r = grow(c, &c->nd.w, cap)) || (r = grow(c, &c->nd.q45, cap)) ||
-      (r = grow(c, &c->nd.q64, cap * 6)) || (r = grow(c, &c->targets, cap)) || (r = grow(c, &c->groups, cap)) ||
+      (r = grow(c, &c->nd.q64, cap * 6)) || (r = grow(c, &c->nd.parent, cap)) || (r = grow(c, &c->nd.upcnt, cap)) ||
+      (r = grow(c, &c->targets, cap)) || (r = grow(c, &c->groups, cap)) ||
       (r = grow(c, &c->group_first, cap)) ||
       (r = grow(c, &c->level_lb, cap / 32 + kLevels + 8)))
     return r;
@@ -376,7 +377,15 @@ void enq_tree(bhg_context* c) {
   launch_topology(c->sys, c->nsys, c->nd, c->keys[0], c->max_leaf, c->level_lb, c->st, c->sms, c->stream);
 }
 
-void enq_moments(bhg_context* c) { launch_moments(c->nd, c->pm, c->st, c->sms, c->stream); }
+// Multipoles in one launch up to this many particles (the per-level launches
+// cost more than the work there), level by level above.  Measured on Plummer
+// spheres (one launch / per level): 0.061 / 0.104 ms at 131k, 0.064 / 0.106
+// at 262k, 0.116 / 0.114 at 524k, 0.200 / 0.144 at 1M, 0.81 / 0.33 at 4M.
+constexpr size_t kMomentsOneLaunchMax = 393216;
+
+void enq_moments(bhg_context* c) {
+  launch_moments(c->nd, c->pm, c->st, c->sms, c->n <= kMomentsOneLaunchMax, c->stream);
+}
 
 void enq_targets(bhg_context* c, uint32_t target_size) {
   cudaStream_t s = c->stream;
@@ -1241,10 +1250,11 @@ int bhg_get_stats(bhg_context* c, bhg_stats* out, int reset) {
   out->depth = c->st_host->max_depth;
   out->sort_passes = kSortPasses;
   // bounds + domain + keys + digit offsets; the sort passes; gather + roots +
-  // one per level; one multipole kernel per level; mark + compact of the
-  // targets and of the groups + first target per group; walk + its
-  // completion count
-  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (kMortonDepth + 1) + 5 + 2 + (c->split_cap ? 1 : 0);
+  // one per level; the multipoles (one kernel, or one per level); mark +
+  // compact of the targets and of the groups + first target per group; walk
+  // (+ its target pass) + its completion count
+  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (c->n <= kMomentsOneLaunchMax ? 1 : kMortonDepth + 1) + 5 +
+                          2 + (c->split_cap ? 1 : 0);
   if (reset) {
     for (double& t : c->tot_ms) t = 0.0;
     c->walks_timed = 0;

@@ -369,6 +369,8 @@ __global__ void k_roots(const SysDev* __restrict__ sys, int nsys, Nodes nd, unsi
   nd.first[s] = leaf ? d.begin : 0u;
   nd.info[s] = (leaf ? 16u : 0u);
   nd.box[s] = make_double4(d.cx, d.cy, d.cz, d.hw);
+  nd.parent[s] = kNoParent;
+  nd.upcnt[s] = 0u;
 }
 
 constexpr int kLevelThreads = 256;  // 8 threads (one per octant) per parent
@@ -458,6 +460,8 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(int depth, Nodes nd, co
         nd.count[ci] = cnt;
         nd.first[ci] = leaf ? start : 0u;
         nd.info[ci] = (leaf ? 16u : 0u) | ((uint32_t)depth << 8);
+        nd.parent[ci] = parent;
+        nd.upcnt[ci] = 0u;
         nd.box[ci] = make_double4((oct & 1) ? __dadd_rn(pbx.x, q) : __dsub_rn(pbx.x, q),
                                   (oct & 2) ? __dadd_rn(pbx.y, q) : __dsub_rn(pbx.y, q),
                                   (oct & 4) ? __dadd_rn(pbx.z, q) : __dsub_rn(pbx.z, q), q);
@@ -562,7 +566,7 @@ __global__ void k_group_first(const uint32_t* __restrict__ groups, const uint32_
 }
 
 // ---------------------------------------------------------------------------
-// a5: multipoles of one level, deepest level first.  finalize_node
+// a5: multipoles, every node after its children (k_moments_up).  finalize_node
 // (flat_tree.h:257-274): raw moments about the cell centre, of the particles
 // (raw_moment_of_particle, multipole.h:52-59) or of the children shifted by
 // the parallel-axis theorem (raw_moment_from_multipole, :92-102), then the
@@ -591,13 +595,10 @@ __device__ __forceinline__ void raw_add(Raw& r, double m, const double d[3], con
   for (int k = 0; k < 6; ++k) r.m2[k] = __dadd_rn(r.m2[k], o[k]);
 }
 
-__global__ void k_moments(int depth, Nodes nd, const double4* __restrict__ pm, const DevState* __restrict__ st) {
-  if (st->status & kStNodeOverflow) return;  // children may lie beyond the slots
-  const uint32_t lb = st->level_begin[depth];
-  const uint32_t lc = depth < (int)st->max_depth ? st->level_count[depth] : 0u;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < lc; k += gridDim.x * blockDim.x) {
-    const uint32_t i = lb + k;
-    if (i >= nd.cap) return;
+// The multipoles and walk record of node i, from its particles (a leaf) or
+// from its children's finished multipoles.
+__device__ void finalize_node(const Nodes& nd, const double4* __restrict__ pm, uint32_t i) {
+  {
     const double4 bx = nd.box[i];
     const double ref[3] = {bx.x, bx.y, bx.z};
     const uint32_t info = nd.info[i];
@@ -614,14 +615,20 @@ __global__ void k_moments(int depth, Nodes nd, const double4* __restrict__ pm, c
     } else {
       const uint32_t f = nd.first[i], nc = info_nchild(info);
       for (uint32_t j = 0; j < nc; ++j) {
-        const double4 cm = nd.mom[f + j];
-        const double* ci = nd.iab + (size_t)(f + j) * 6;
-        const double d[3] = {__dsub_rn(cm.x, ref[0]), __dsub_rn(cm.y, ref[1]), __dsub_rn(cm.z, ref[2])};
+        // the children were written by other threads of this launch: read
+        // them from L2 (an L1 line may be older than their fence)
+        const double2* cp = reinterpret_cast<const double2*>(nd.mom + f + j);
+        const double2 c01 = __ldcg(cp), c23 = __ldcg(cp + 1);
+        const double2* ip = reinterpret_cast<const double2*>(nd.iab + (size_t)(f + j) * 6);
+        const double2 i01 = __ldcg(ip), i23 = __ldcg(ip + 1), i45 = __ldcg(ip + 2);
+        const double ci[6] = {i01.x, i01.y, i23.x, i23.y, i45.x, i45.y};
+        const double cmw = c23.y;
+        const double d[3] = {__dsub_rn(c01.x, ref[0]), __dsub_rn(c01.y, ref[1]), __dsub_rn(c23.x, ref[2])};
         double o[6];
-        outer_sym_rn(d, cm.w, o);
+        outer_sym_rn(d, cmw, o);
 #pragma unroll
         for (int t = 0; t < 6; ++t) o[t] = __dadd_rn(ci[t], o[t]);
-        raw_add(r, cm.w, d, o);
+        raw_add(r, cmw, d, o);
       }
     }
     // finalize_raw_moment
@@ -662,6 +669,43 @@ __global__ void k_moments(int depth, Nodes nd, const double4* __restrict__ pm, c
     w.q[3] = (float)q[3];
     nd.w[i] = w;
     nd.q45[i] = make_float2((float)q[4], (float)q[5]);
+  }
+}
+
+// a5 level by level, deepest level first: one launch per level.
+__global__ void k_moments(int depth, Nodes nd, const double4* __restrict__ pm, const DevState* __restrict__ st) {
+  if (st->status & kStNodeOverflow) return;  // children may lie beyond the slots
+  const uint32_t lb = st->level_begin[depth];
+  const uint32_t lc = depth < (int)st->max_depth ? st->level_count[depth] : 0u;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < lc; k += gridDim.x * blockDim.x) {
+    const uint32_t i = lb + k;
+    if (i >= nd.cap) return;
+    finalize_node(nd, pm, i);
+  }
+}
+
+// a5 in one launch: every leaf is finalized by one thread, which then climbs
+// while it is the last of its parent's children to finish (a counter per
+// node), so every node is finalized once, after all its children, and sums
+// its children in order as finalize_node does level by level.  No thread
+// waits for another.
+__global__ void k_moments_up(Nodes nd, const double4* __restrict__ pm, const DevState* __restrict__ st) {
+  if (st->status & kStNodeOverflow) return;  // children may lie beyond the slots
+  const uint32_t nn = min(st->n_nodes, nd.cap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    if (!info_leaf(nd.info[i])) continue;
+    uint32_t node = i;
+    finalize_node(nd, pm, node);
+    for (;;) {
+      const uint32_t par = nd.parent[node];
+      if (par == kNoParent) break;
+      __threadfence();  // this node's multipoles before the count
+      const uint32_t done = atomicAdd(&nd.upcnt[par], 1u) + 1u;
+      if (done < info_nchild(nd.info[par])) break;  // a sibling finishes the parent
+      __threadfence();
+      finalize_node(nd, pm, par);
+      node = par;
+    }
   }
 }
 
@@ -720,8 +764,12 @@ void launch_targets(const Nodes& nd, uint32_t lim, uint32_t group_lim, uint32_t 
   k_group_first<<<sms * 2, 256, 0, s>>>(groups, targets, nd.begin, st, first_target);
 }
 
-void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, cudaStream_t s) {
-  for (int d = kMortonDepth; d >= 0; --d) k_moments<<<sms * 4, 128, 0, s>>>(d, nd, pm, st);
+void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, bool one_launch, cudaStream_t s) {
+  if (one_launch) {
+    k_moments_up<<<sms * 4, 128, 0, s>>>(nd, pm, st);
+  } else {
+    for (int d = kMortonDepth; d >= 0; --d) k_moments<<<sms * 4, 128, 0, s>>>(d, nd, pm, st);
+  }
 }
 
 }  // namespace bhg

@@ -136,8 +136,11 @@ struct Nodes {
   WNode* w;         // walk records
   float2* q45;      // FP32 traceless quadrupole xz, yz
   double* q64;      // 6 per node: FP64 traceless quadrupole (the FP64 walk)
+  uint32_t* parent; // parent slot (kNoParent for a root)
+  uint32_t* upcnt;  // children whose multipoles are done (the upward pass)
   uint32_t cap;     // node slots
 };
+constexpr uint32_t kNoParent = 0xffffffffu;
 
 // Kernel-launch helpers shared by the .cu files (defined in bhg_build.cu).
 constexpr int kTile = 4096;  // particles per radix-sort / bounds tile

@@ -31,7 +31,9 @@ void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_
 void launch_targets(const Nodes& nd, uint32_t lim, uint32_t group_lim, uint32_t n, uint32_t* mark, uint32_t* targets,
                     uint32_t* groups, uint32_t* first_target, uint32_t* lookback, DevState* st, int sms,
                     cudaStream_t s);
-void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, cudaStream_t s);
+// one_launch: k_moments_up (one kernel, children-first by counters) instead of
+// one kernel per level; the same bits either way
+void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, bool one_launch, cudaStream_t s);
 
 struct WalkArgs {
   const WNode* w;

@@ -56,6 +56,21 @@ def test_build_bit_exact(gpu, oracle, name, make, max_leaf, gs, ts, theta, eps2)
         assert np.array_equal(g[k], np.asarray(t[k][:n])), f"node {k} not bit-identical"
 
 
+def test_build_bit_exact_per_level_multipoles(gpu, oracle):
+    """Above 393,216 particles the multipoles run one launch per level instead
+    of the one-launch upward pass the small cases take: the same bits."""
+    parts = bhg.plummer(450000, 12)[0]
+    dom, sk, perm, mp, t = _oracle_build(oracle, parts, 16)
+    gpu.upload(parts)
+    gpu.build_tree(16, 256)
+    gpu.compute_multipoles()
+    g = gpu.tree()
+    n = t["n"]
+    assert g["n"] == n
+    for k in ("begin", "count", "first_child", "nchild", "leaf", "depth", "center", "hw", "mass", "com", "iab"):
+        assert np.array_equal(g[k], np.asarray(t[k][:n])), f"node {k} differs"
+
+
 @pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-12), (bhg.PRECISION_SPLIT, 1e-5)])
 @pytest.mark.parametrize("name,make,max_leaf,gs,ts,theta,eps2", CASES, ids=[c[0] for c in CASES])
 def test_walk_matches_oracle(gpu, oracle, name, make, max_leaf, gs, ts, theta, eps2, precision, tol):
