@@ -596,7 +596,9 @@ __device__ __forceinline__ void raw_add(Raw& r, double m, const double d[3], con
 }
 
 // The multipoles and walk record of node i, from its particles (a leaf) or
-// from its children's finished multipoles.
+// from its children's finished multipoles (read through L2 when other
+// threads of the same launch wrote them: FROM_L2).
+template <bool FROM_L2>
 __device__ void finalize_node(const Nodes& nd, const double4* __restrict__ pm, uint32_t i) {
   {
     const double4 bx = nd.box[i];
@@ -615,12 +617,13 @@ __device__ void finalize_node(const Nodes& nd, const double4* __restrict__ pm, u
     } else {
       const uint32_t f = nd.first[i], nc = info_nchild(info);
       for (uint32_t j = 0; j < nc; ++j) {
-        // the children were written by other threads of this launch: read
-        // them from L2 (an L1 line may be older than their fence)
+        // children written by other threads of this launch are read from L2
+        // (an L1 line may be older than their fence)
         const double2* cp = reinterpret_cast<const double2*>(nd.mom + f + j);
-        const double2 c01 = __ldcg(cp), c23 = __ldcg(cp + 1);
         const double2* ip = reinterpret_cast<const double2*>(nd.iab + (size_t)(f + j) * 6);
-        const double2 i01 = __ldcg(ip), i23 = __ldcg(ip + 1), i45 = __ldcg(ip + 2);
+        const double2 c01 = FROM_L2 ? __ldcg(cp) : cp[0], c23 = FROM_L2 ? __ldcg(cp + 1) : cp[1];
+        const double2 i01 = FROM_L2 ? __ldcg(ip) : ip[0], i23 = FROM_L2 ? __ldcg(ip + 1) : ip[1];
+        const double2 i45 = FROM_L2 ? __ldcg(ip + 2) : ip[2];
         const double ci[6] = {i01.x, i01.y, i23.x, i23.y, i45.x, i45.y};
         const double cmw = c23.y;
         const double d[3] = {__dsub_rn(c01.x, ref[0]), __dsub_rn(c01.y, ref[1]), __dsub_rn(c23.x, ref[2])};
@@ -680,7 +683,7 @@ __global__ void k_moments(int depth, Nodes nd, const double4* __restrict__ pm, c
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < lc; k += gridDim.x * blockDim.x) {
     const uint32_t i = lb + k;
     if (i >= nd.cap) return;
-    finalize_node(nd, pm, i);
+    finalize_node<false>(nd, pm, i);
   }
 }
 
@@ -695,7 +698,7 @@ __global__ void k_moments_up(Nodes nd, const double4* __restrict__ pm, const Dev
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
     if (!info_leaf(nd.info[i])) continue;
     uint32_t node = i;
-    finalize_node(nd, pm, node);
+    finalize_node<true>(nd, pm, node);
     for (;;) {
       const uint32_t par = nd.parent[node];
       if (par == kNoParent) break;
@@ -703,7 +706,7 @@ __global__ void k_moments_up(Nodes nd, const double4* __restrict__ pm, const Dev
       const uint32_t done = atomicAdd(&nd.upcnt[par], 1u) + 1u;
       if (done < info_nchild(nd.info[par])) break;  // a sibling finishes the parent
       __threadfence();
-      finalize_node(nd, pm, par);
+      finalize_node<true>(nd, pm, par);
       node = par;
     }
   }
