@@ -23,7 +23,7 @@ PARTICLE = np.dtype(
     [("id", "<u4"), ("pad", "<u4"), ("mass", "<f8"), ("pos", "<f8", (3,)), ("vel", "<f8", (3,))]
 )
 
-OK, EINVAL, ECUDA, ENOMEM, ENONFINITE, ESTATE, EDEVICE, ECANCELLED = range(8)
+OK, EINVAL, ECUDA, ENOMEM, ENONFINITE, ESTATE, EDEVICE, ECANCELLED, EAGAIN = range(9)
 PRECISION_SPLIT, PRECISION_FP64 = 0, 1
 EXPORT_KEYS, EXPORT_PERM, EXPORT_NODES_U32, EXPORT_NODES_F64, EXPORT_DOMAINS, EXPORT_TARGETS, EXPORT_ACCEL = range(1, 8)
 
@@ -34,6 +34,7 @@ EXPORTED = (
     "bhg_add_generated", "bhg_remove_systems", "bhg_num_systems", "bhg_system_ids", "bhg_upload_csv",
     "bhg_upload_csv_device", "bhg_add_csv", "bhg_snapshot_vtk", "bhg_build_tree",
     "bhg_compute_multipoles", "bhg_walk_forces", "bhg_integrate", "bhg_step", "bhg_step_systems",
+    "bhg_step_systems_async", "bhg_download_async", "bhg_sync",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
     "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
     "bhg_measure_fp32_peak",
@@ -111,6 +112,9 @@ def lib() -> C.CDLL:
         "bhg_integrate": ([vp, f64, f64], i32),
         "bhg_step": ([vp, C.POINTER(ForceParams), C.c_uint, u32, u32, f64, f64], i32),
         "bhg_step_systems": ([vp, C.POINTER(ForceParams), C.c_uint, u32, u32], i32),
+        "bhg_step_systems_async": ([vp, C.POINTER(ForceParams), C.c_uint, u32, u32], i32),
+        "bhg_download_async": ([vp, vp], i32),
+        "bhg_sync": ([vp], i32),
         "bhg_run_schedule": ([vp, C.POINTER(ForceParams), C.c_uint, u32, u32, f64, i32], i32),
         "bhg_set_system_params": ([vp, vp, vp, vp, vp], i32),
         "bhg_get_stats": ([vp, C.POINTER(Stats), i32], i32),
@@ -326,6 +330,20 @@ class Context:
 
     def step_systems(self, fp, max_leaf, group_size, target_size):
         self._ck(self.L.bhg_step_systems(self.h, C.byref(fp), max_leaf, group_size, target_size))
+
+    def step_systems_async(self, fp, max_leaf, group_size, target_size):
+        """Enqueues one evaluation of every system and returns; sync() reports it."""
+        self._ck(self.L.bhg_step_systems_async(self.h, C.byref(fp), max_leaf, group_size, target_size))
+
+    def download_async(self, out_ptr: int):
+        """Enqueues the copy of the particles to host address out_ptr (pinned
+        memory: the call does not block); valid after sync()."""
+        self._ck(self.L.bhg_download_async(self.h, C.c_void_p(out_ptr)))
+
+    def sync(self):
+        """Waits for the context's stream; raises for the enqueued evaluations
+        that did not run (EAGAIN: node slots regrown, run them again)."""
+        self._ck(self.L.bhg_sync(self.h))
 
     def run_schedule(self, fp, max_leaf, group_size, target_size, dt, steps):
         self._ck(self.L.bhg_run_schedule(self.h, C.byref(fp), max_leaf, group_size, target_size, dt, steps))

@@ -87,6 +87,11 @@ struct bhg_context {
   double last_walk_ms = 0.0;
   uint32_t walks_timed = 0;
 
+  // evaluations enqueued by bhg_step_systems_async since the last bhg_sync,
+  // and the count of finished evaluations before them
+  int async_pending = 0;
+  uint32_t async_base = 0;
+
   // captured graphs, one per phase
   cudaGraphExec_t graph[kPhases] = {};
   std::string graph_key[kPhases];
@@ -288,7 +293,14 @@ int ensure_walk_scratch(bhg_context* c, int grid) {
 // the buffers for them (the state's first c->n particles survive a growth)
 // and resets the per-step device state.  Per-system parameters stay with
 // their systems; new systems get the defaults.
+int finish_async(bhg_context* c);
+int read_state(bhg_context* c);
+
 int relayout(bhg_context* c) {
+  if (c->async_pending) {  // the systems change: report the enqueued evaluations first
+    int r = read_state(c);
+    if (r || (r = finish_async(c))) return r;
+  }
   const size_t nsys = c->counts.size();
   size_t n = 0, ntiles = 0;
   for (size_t s = 0; s < nsys; ++s) {
@@ -1157,6 +1169,36 @@ int prepare_step(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, 
   return BHG_OK;
 }
 
+// The node slots an overflowed build asked for, with room to spare.
+size_t regrown_nodes(const bhg_context* c) {
+  return std::max<size_t>(2 * c->cap_nodes, (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64);
+}
+
+// Reports the evaluations enqueued by bhg_step_systems_async (the device
+// state has just been read).
+int finish_async(bhg_context* c) {
+  const int pending = c->async_pending;
+  c->async_pending = 0;
+  if (pending == 0) return BHG_OK;
+  const uint32_t ran = c->st_host->evals_ok - c->async_base;
+  const uint32_t st = c->st_host->status;
+  if (st == 0) {
+    c->walked = true;
+    c->built = c->moments = false;
+    return BHG_OK;
+  }
+  int r;
+  if (st & kStNodeOverflow) {
+    if ((r = clear_status(c)) || (r = ensure_nodes(c, regrown_nodes(c))) || (r = ensure_walk_scratch(c, walk_grid(c))))
+      return r;
+    return fail(c, BHG_EAGAIN, std::to_string(ran) + " of " + std::to_string(pending) +
+                                   " evaluations ran: the octree outgrew its node slots (now grown)");
+  }
+  r = check_status(c);
+  clear_status(c);
+  return r;
+}
+
 // Runs evaluations i0 .. i1-1 of a schedule given by kick/drift per
 // evaluation; on a node overflow grows the slots and resumes from the
 // evaluation that failed (its walk was skipped, so the state is intact).
@@ -1165,6 +1207,7 @@ int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<
   for (int attempt = 0; attempt < 8; ++attempt) {
     int r;
     if ((r = read_state(c))) return r;
+    if (c->async_pending && (r = finish_async(c))) return r;
     const uint32_t base = c->st_host->evals_ok;
     for (size_t i = next; i < kd.size(); ++i) {
       if (!keep) {
@@ -1184,8 +1227,8 @@ int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<
     }
     if (c->st_host->status & kStNodeOverflow) {
       next += done;
-      size_t need = std::max<size_t>(2 * c->cap_nodes, (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64);
-      if ((r = clear_status(c)) || (r = ensure_nodes(c, need)) || (r = ensure_walk_scratch(c, walk_grid(c)))) return r;
+      if ((r = clear_status(c)) || (r = ensure_nodes(c, regrown_nodes(c))) || (r = ensure_walk_scratch(c, walk_grid(c))))
+        return r;
       continue;
     }
     r = check_status(c);
@@ -1213,6 +1256,32 @@ int bhg_step_systems(bhg_context* c, const bhg_force_params* fp, unsigned max_le
   int r = prepare_step(c, fp, max_leaf, group_size, 0.0, 0.0, true);
   if (r) return r;
   return run_evals(c, target_size, {{0.0, 0.0}}, true);
+}
+
+int bhg_step_systems_async(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
+                           uint32_t target_size) {
+  if (!c) return BHG_EINVAL;
+  int r = prepare_step(c, fp, max_leaf, group_size, 0.0, 0.0, true);
+  if (r) return r;
+  if (c->async_pending == 0) c->async_base = c->st_host->evals_ok;  // current: read at the last sync
+  if ((r = push_params(c)) || (r = enq_step(c, target_size))) return r;
+  ++c->async_pending;
+  return BHG_OK;
+}
+
+int bhg_download_async(bhg_context* c, bh_particle64* out) {
+  if (!c || !out) return fail(c, BHG_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  CK(cudaMemcpyAsync(out, c->part, c->n * sizeof(Particle), cudaMemcpyDeviceToHost, c->stream));
+  return BHG_OK;
+}
+
+int bhg_sync(bhg_context* c) {
+  if (!c) return BHG_EINVAL;
+  cudaSetDevice(c->device);
+  int r = read_state(c);
+  if (r) return r;
+  return finish_async(c);
 }
 
 int bhg_run_schedule(bhg_context* c, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,

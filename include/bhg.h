@@ -38,6 +38,7 @@ extern "C" {
 #define BHG_ESTATE 5      /* call out of order (e.g. walk before build) */
 #define BHG_EDEVICE 6     /* a kernel reported an internal limit (see message) */
 #define BHG_ECANCELLED 7  /* serving: the request was cancelled */
+#define BHG_EAGAIN 8      /* bhg_sync: not every enqueued evaluation ran (see message); run them again */
 
 /* bh::Particle (particle.h:7-24): 64 bytes, 4 bytes of padding after id. */
 typedef struct bh_particle64 {
@@ -212,6 +213,21 @@ int bhg_step(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, ui
  * quadrupole switch and the precision). */
 int bhg_step_systems(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
                      uint32_t target_size);
+/* Asynchronous forms, for overlapping one context's copies with another's
+ * evaluations (several contexts, each on its own stream, each holding some
+ * of the systems: a system's result does not depend on the others in its
+ * context).  bhg_step_systems_async enqueues the evaluation and returns;
+ * bhg_download_async enqueues the copy (into pinned memory it does not block;
+ * `out` must stay valid until bhg_sync).  bhg_sync waits for the context's
+ * stream and reports the enqueued evaluations: BHG_OK; BHG_EAGAIN when the
+ * octree outgrew its node slots (they are grown: the state is as after the
+ * last evaluation that ran, and the message says how many ran); or the
+ * error that stopped them.  A blocking call after async ones reports them
+ * first, as bhg_sync would. */
+int bhg_step_systems_async(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
+                           uint32_t target_size);
+int bhg_download_async(bhg_context* ctx, bh_particle64* out);
+int bhg_sync(bhg_context* ctx);
 /* The leapfrog schedule of main.cc:199-246: a (dt/2, dt) evaluation,
  * steps-1 (dt, dt) evaluations and a closing (dt/2, 0) one. */
 int bhg_run_schedule(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,

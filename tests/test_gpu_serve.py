@@ -173,3 +173,64 @@ def test_suspended_request_resumes_bit_for_bit(precision):
     assert rep["completed"] == 3
     for r in reqs:
         assert srv.results[r.rid].tobytes() == run_alone(r, precision).tobytes()
+
+
+def test_pipeline_equals_one_context():
+    """Systems stepped through three contexts with asynchronous steps and
+    downloads from pinned memory come back as one context returns them."""
+    import torch
+
+    from bhg.pipeline import Pipeline
+
+    systems = [bhg.plummer(n, 300 + i)[0] for i, n in enumerate((3000, 9000, 1500, 20000, 6000, 700, 12000))]
+    counts = [len(s) for s in systems]
+    th = np.array([0.5, 0.6, 0.4, 0.5, 0.7, 0.5, 0.5])
+    e2 = np.array([1e-4, 1e-4, 4e-4, 1e-4, 1e-4, 2.5e-5, 1e-4])
+    kick, drift = np.full(7, 0.01), np.full(7, 0.02)
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, bhg.PRECISION_SPLIT)
+    with bhg.Context(device=0) as one:
+        one.upload_systems(systems)
+        for _ in range(2):
+            one.set_system_params(theta=th, eps2=e2, kick_dt=kick, drift_dt=drift)
+            one.step_systems(fp, 16, 256, 16)
+        want = one.download()
+    n = sum(counts)
+    buf = torch.empty(n * bhg.PARTICLE.itemsize, dtype=torch.uint8, pin_memory=True)
+    host = np.frombuffer(buf.numpy(), dtype=bhg.PARTICLE)
+    host[:] = np.concatenate(systems)
+    with Pipeline(counts, parts=3) as pl:
+        assert len(pl.ctxs) == 3
+        for _ in range(2):
+            pl.step(buf.data_ptr(), fp, 16, 256, 16, th, e2, kick, drift)
+    assert host.tobytes() == want.tobytes()
+
+
+def test_async_step_reports_node_overflow():
+    """An asynchronous evaluation whose octree outgrows the node slots is
+    reported by bhg_sync as EAGAIN with the slots grown; run again it gives
+    what the blocking step gives."""
+    from helpers import cube
+
+    parts = cube(4000, 12, spread=10.0)
+    parts["pos"] = np.repeat(parts["pos"][::8], 8, axis=0) + np.random.default_rng(3).uniform(-1e-7, 1e-7, (4000, 3))
+    fp = bhg.Context.params(0.5, 1e-8, 1.0, True, bhg.PRECISION_FP64)
+    with bhg.Context(device=0) as ctx:
+        ctx.upload(parts)
+        ctx.set_system_params(theta=[0.5], eps2=[1e-8], kick_dt=[0.01], drift_dt=[0.01])
+        ctx.step_systems_async(fp, 1, 64, 0)
+        with pytest.raises(bhg.BhgError) as e:
+            ctx.sync()
+        assert e.value.code == bhg.EAGAIN
+        assert ctx.download().tobytes() == parts.tobytes()  # nothing moved
+        for _ in range(8):  # each overflow grows the slots past the level it reached
+            ctx.step_systems_async(fp, 1, 64, 0)
+            try:
+                ctx.sync()
+                break
+            except bhg.BhgError as again:
+                assert again.code == bhg.EAGAIN
+        got = ctx.download()
+    with bhg.Context(device=0) as ref:
+        ref.upload(parts)
+        ref.step(fp, 1, 64, 0, 0.01, 0.01)
+        assert ref.download().tobytes() == got.tobytes()

@@ -155,3 +155,15 @@ def test_cancel_active_and_queued(monkeypatch):
     rep = srv.run(reqs[2:], realtime=False)
     assert rep["cancelled"] == 2 and rep["completed"] == 2
     assert srv.ctx.sizes == {}
+
+
+def test_pipeline_split_is_contiguous_and_balanced():
+    from bhg.pipeline import split_systems
+
+    assert split_systems([10, 10, 10, 10], 2) == [(0, 2), (2, 4)]
+    assert split_systems([10, 10, 10, 10], 3) == [(0, 2), (2, 3), (3, 4)]
+    assert split_systems([100, 1, 1, 1], 2) == [(0, 1), (1, 4)]
+    assert split_systems([5, 5], 8) == [(0, 1), (1, 2)]
+    runs = split_systems(list(range(1, 101)), 4)
+    assert runs[0][0] == 0 and runs[-1][1] == 100
+    assert all(a < b for a, b in runs) and all(runs[i][1] == runs[i + 1][0] for i in range(3))
