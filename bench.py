@@ -780,6 +780,19 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
         except (OSError, subprocess.CalledProcessError) as e:
             out["cpu_baseline"] = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "reference",
                                    "sample": f"unavailable: {e}"}
+    if rig.rank == 0:
+        # a served system's forces are those of the system alone, bit for bit
+        # (tests/test_gpu_serve.py): the force error of the largest theta-0.5
+        # request among the stream's first 64, its initial conditions made by
+        # the same device generator
+        pick = max((r for r in reqs[:64] if r.theta == 0.5), key=lambda r: r.n, default=None)
+        if pick is not None:
+            with bhg.Context(device=rig.local) as c:
+                c.add_generated(pick.spheres(), pick.seed, id0=0)
+                parts = c.download()
+                fp = bhg.Context.params(0.5, pick.eps ** 2, 1.0, True, bhg.PRECISION_SPLIT)
+                out["force_error"] = force_error(c, parts, fp, w["max_leaf"], w["group"], w["max_leaf"], pick.eps ** 2)
+            out["force_error"]["system"] = f"request {pick.rid}: {pick.kind}, N={pick.n}, theta 0.5"
     out["config_extra"] = {"mean_particles_per_tick": n_eval}
     return out
 
