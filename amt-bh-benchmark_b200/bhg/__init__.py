@@ -30,7 +30,7 @@ EXPORT_KEYS, EXPORT_PERM, EXPORT_NODES_U32, EXPORT_NODES_F64, EXPORT_DOMAINS, EX
 #: Every entry point include/bhg.h declares.
 EXPORTED = (
     "bhg_create", "bhg_destroy", "bhg_last_error", "bhg_set_stream", "bhg_upload", "bhg_upload_device",
-    "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_add_system",
+    "bhg_upload_systems", "bhg_download", "bhg_download_device", "bhg_num_particles", "bhg_reserve", "bhg_add_system",
     "bhg_add_generated", "bhg_remove_systems", "bhg_num_systems", "bhg_system_ids", "bhg_upload_csv",
     "bhg_upload_csv_device", "bhg_add_csv", "bhg_snapshot_vtk", "bhg_build_tree",
     "bhg_compute_multipoles", "bhg_walk_forces", "bhg_integrate", "bhg_step", "bhg_step_systems",
@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         "bhg_download": ([vp, vp], i32),
         "bhg_download_device": ([vp, vp], i32),
         "bhg_num_particles": ([vp], sz),
+        "bhg_reserve": ([vp, sz, sz], i32),
         "bhg_add_system": ([vp, vp, sz, C.POINTER(u64)], i32),
         "bhg_add_generated": ([vp, vp, i32, u64, u32, C.POINTER(u64)], i32),
         "bhg_remove_systems": ([vp, vp, sz, vp], i32),
@@ -221,6 +222,11 @@ class Context:
         counts = np.array([len(s) for s in systems], np.uint64)
         self._ck(self.L.bhg_upload_systems(self.h, _p(parts), _p(counts), len(counts)))
         self.n = len(parts)
+
+    def reserve(self, particles, systems):
+        """Grows the buffers now for up to `particles` particles in up to
+        `systems` systems (no allocation or state copy when systems join later)."""
+        self._ck(self.L.bhg_reserve(self.h, int(particles), int(systems)))
 
     def add_system(self, parts) -> int:
         """Appends one system (host particles); returns its handle."""

@@ -28,6 +28,7 @@ from . import ENOMEM, PRECISION_SPLIT, BhgError, Context
 #: (128), sources (32), sort keys and values (24), marks (4), ~0.45 node
 #: slots of 264 bytes (~119), rounded up
 BYTES_PER_PARTICLE = 320
+RESERVED_SYSTEMS = 4096  # per-system tables sized up front by Server
 
 
 @dataclasses.dataclass
@@ -108,6 +109,14 @@ class Server:
         # buffers' growth slack and the state's second copy while it grows
         self.ctx = Context(device=device, hbm_budget=int(hbm_budget * 1.15) + (512 << 20))
         self.budget = hbm_budget
+        # the buffers for a full batch up front: admissions then neither
+        # allocate nor copy the resident state (without the memory for it
+        # they grow as systems join)
+        try:
+            self.ctx.reserve(int(hbm_budget // BYTES_PER_PARTICLE), RESERVED_SYSTEMS)
+        except BhgError as e:
+            if e.code != ENOMEM:
+                raise
         self.max_batch = max_batch_particles
         self.max_leaf, self.group_size, self.precision = max_leaf, group_size, precision
         self.keep_results = keep_results
@@ -128,6 +137,8 @@ class Server:
         self.hold = False  # after a preemption: admit nothing until a request completes
         self.saved: dict[int, Checkpoint] = {}  # suspended requests, resumed at their next admission
         self.cancelled: set[int] = set()
+        self.admit_s = 0.0  # wall seconds spent adding systems (admissions, resumptions)
+        self.retire_s = 0.0  # wall seconds spent taking finished systems off (with their copies)
         self.n_cancelled = 0
 
     def close(self):
@@ -144,6 +155,7 @@ class Server:
             if self.hold or after * BYTES_PER_PARTICLE > self.budget or (self.max_batch and after > self.max_batch):
                 return False
         ck = self.saved.get(req.rid)
+        t0 = time.perf_counter()
         try:
             if ck is not None:  # resumed where it was suspended
                 h = self.ctx.add_system(ck.particles)
@@ -155,6 +167,8 @@ class Server:
             if e.code == ENOMEM and self.active:  # no room until some request leaves
                 return False
             raise
+        finally:
+            self.admit_s += time.perf_counter() - t0
         if ck is not None:
             del self.saved[req.rid]
             self.active.append(_Active(req, h, ck.evals_done, now, ck.counted))
@@ -238,6 +252,7 @@ class Server:
             if a.evals_done == a.req.steps + 1:
                 done.append(a)
         if done:
+            t1 = time.perf_counter()
             for a in done:  # snapshots are formatted on the device before the systems leave
                 if a.req.snapshot:
                     self.snapshots[a.req.rid] = self.ctx.snapshot_vtk(a.handle)
@@ -252,6 +267,7 @@ class Server:
                 if self.on_result is not None:
                     self.on_result(a.req.rid, parts[j])
             self.completed += len(done)
+            self.retire_s += time.perf_counter() - t1
             self.hold = False
             gone = {id(a) for a in done}
             self.active = [a for a in self.active if id(a) not in gone]
@@ -297,7 +313,8 @@ class Server:
         return {"wall_s": wall_s, "admitted": self.admitted, "completed": self.completed,
                 "in_flight": len(self.active), "queued": queued, "preempted": self.preempted,
                 "cancelled": self.n_cancelled,
-                "ticks": len(self.tick_ms), "particle_steps": self.particle_steps,
+                "ticks": len(self.tick_ms), "tick_s": sum(self.tick_ms) / 1000.0, "admit_s": self.admit_s,
+                "retire_s": self.retire_s, "particle_steps": self.particle_steps,
                 "particle_steps_per_s": self.particle_steps / wall_s if wall_s > 0 else 0.0,
                 "step_latency_ms_p50": float(np.percentile(lat, 50)),
                 "step_latency_ms_p99": float(np.percentile(lat, 99)),

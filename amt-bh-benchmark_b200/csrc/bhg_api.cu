@@ -736,6 +736,19 @@ static int add_system_impl(bhg_context* c, size_t n, uint64_t* id, F fill) {
 
 extern "C" {
 
+int bhg_reserve(bhg_context* c, size_t particles, size_t systems) {
+  if (!c) return BHG_EINVAL;
+  if (particles >= (1ull << 30)) return fail(c, BHG_EINVAL, "more than 2^30 - 1 particles");
+  if (systems == 0 || systems > 65535) return fail(c, BHG_EINVAL, "systems must be in 1 .. 65535");
+  cudaSetDevice(c->device);
+  const size_t n = std::max(particles, c->n);
+  const size_t nsys = std::max(systems, c->counts.size());
+  int r;
+  if ((r = ensure_particles(c, n, (int)nsys, n / kTile + nsys)) || (r = ensure_nodes(c, node_estimate(n, (int)nsys, 16))))
+    return r;
+  return BHG_OK;
+}
+
 int bhg_add_system(bhg_context* c, const bh_particle64* p, size_t n, uint64_t* id) {
   if (!c) return BHG_EINVAL;
   if (!p) return fail(c, BHG_EINVAL, "null particles");

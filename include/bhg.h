@@ -137,6 +137,12 @@ typedef struct bhg_sphere {
   double bulk[3];
 } bhg_sphere;
 
+/* Grows the context's buffers now for up to `particles` particles in up to
+ * `systems` systems, with the node slots they bring at max_leaf 16, so that
+ * systems added later within those sizes neither allocate nor copy the
+ * resident state.  Counts against the HBM budget (BHG_ENOMEM past it). */
+int bhg_reserve(bhg_context* ctx, size_t particles, size_t systems);
+
 /* Appends one system of n particles from host memory; its handle goes to
  * *id.  The resident systems keep their particles and parameters; the new
  * one starts with theta 0.5, eps2 0 and no kick/drift (bhg_set_system_params). */

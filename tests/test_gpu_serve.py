@@ -234,3 +234,29 @@ def test_async_step_reports_node_overflow():
         ref.upload(parts)
         ref.step(fp, 1, 64, 0, 0.01, 0.01)
         assert ref.download().tobytes() == got.tobytes()
+
+
+def test_reserve_then_add_equals_growth():
+    """bhg_reserve sizes the buffers up front: systems added afterwards step
+    to the same bits as in a context that grew for them; past the HBM budget
+    the reservation is a clean ENOMEM."""
+    systems = [bhg.plummer(n, 400 + i)[0] for i, n in enumerate((5000, 12000, 3000))]
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, bhg.PRECISION_SPLIT)
+    out = []
+    for reserve in (True, False):
+        with bhg.Context(device=0) as ctx:
+            if reserve:
+                ctx.reserve(40000, 8)
+            for s in systems:
+                ctx.add_system(s)
+            ctx.set_system_params(theta=np.full(3, 0.5), eps2=np.full(3, 1e-4), kick_dt=np.full(3, 0.01),
+                                  drift_dt=np.full(3, 0.01))
+            ctx.step_systems(fp, 16, 256, 16)
+            out.append(ctx.download())
+    assert out[0].tobytes() == out[1].tobytes()
+    with bhg.Context(device=0, hbm_budget=64 << 20) as small:
+        with pytest.raises(bhg.BhgError) as e:
+            small.reserve(10_000_000, 8)
+        assert e.value.code == bhg.ENOMEM
+        small.add_system(systems[0])  # still usable
+        assert small.download().tobytes() == systems[0].tobytes()

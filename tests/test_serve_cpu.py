@@ -38,6 +38,10 @@ class _FakeContext:
     def __init__(self, device=0, hbm_budget=0):
         self.sizes = {}
         self.next = 1
+        self.reserved = None
+
+    def reserve(self, particles, systems):
+        self.reserved = (particles, systems)
 
     @staticmethod
     def params(*a):
