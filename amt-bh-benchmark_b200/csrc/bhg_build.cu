@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(256) k_digit_offsets(const SysDev* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// a3: one LSD radix pass (8-bit digit), one tile of kTile keys per block.
+// a3: one LSD radix pass (8-bit digit), one tile of keys per block.
 // Within a warp, equal digits are ranked with __match_any_sync in item order;
 // warps are combined per digit; tiles of the same system chain through a
 // decoupled look-back; keys are then staged in shared memory in digit order
@@ -229,9 +229,14 @@ __global__ void __launch_bounds__(256) k_digit_offsets(const SysDev* __restrict_
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = kTile / kSortThreads;  // 16 per thread
-constexpr size_t kSortSmem = (size_t)kTile * 8 + (size_t)kTile * 4 + (size_t)kSortWarps * 256 * 4 + 2 * 256 * 4 + 64;
+// keys per thread: 16 (4096-key tiles) or, for small problems, 4 (1024-key
+// tiles: four times the blocks per pass)
+template <int ITEMS>
+constexpr size_t sort_smem() {
+  return (size_t)kSortThreads * ITEMS * 12 + (size_t)kSortWarps * 256 * 4 + 2 * 256 * 4 + 64;
+}
 
+template <int kSortItems>
 __global__ void __launch_bounds__(kSortThreads) k_sort_pass(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                             uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                             int pass, const Tile* __restrict__ tiles,
@@ -239,8 +244,9 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_pass(const uint64_t* __re
                                                             DevState* st) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);
-  uint32_t* s_vals = reinterpret_cast<uint32_t*>(smem + (size_t)kTile * 8);
-  uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem + (size_t)kTile * 12);  // [warp][256]
+  constexpr int kSortTile = kSortThreads * kSortItems;
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(smem + (size_t)kSortTile * 8);
+  uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem + (size_t)kSortTile * 12);  // [warp][256]
   uint32_t* s_lbase = s_whist + kSortWarps * 256;
   uint32_t* s_gbase = s_lbase + 256;
   uint32_t* s_misc = s_gbase + 256;
@@ -721,7 +727,8 @@ __global__ void k_moments_up(Nodes nd, const double4* __restrict__ pm, const Dev
 void set_build_attributes() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
+  cudaFuncSetAttribute(k_sort_pass<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem<16>());
+  cudaFuncSetAttribute(k_sort_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem<4>());
   done = true;
 }
 
@@ -738,9 +745,12 @@ void launch_keys(const Particle* p, const Tile* tiles, int ntiles, const SysDev*
 }
 
 void launch_sort_pass(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout, int pass,
-                      const Tile* tiles, int ntiles, const uint32_t* offs, uint32_t* lookback, DevState* st,
-                      cudaStream_t s) {
-  k_sort_pass<<<ntiles, kSortThreads, kSortSmem, s>>>(kin, vin, kout, vout, pass, tiles, offs, lookback, st);
+                      const Tile* tiles, int ntiles, int tile_keys, const uint32_t* offs, uint32_t* lookback,
+                      DevState* st, cudaStream_t s) {
+  if (tile_keys == kSortThreads * 4)
+    k_sort_pass<4><<<ntiles, kSortThreads, sort_smem<4>(), s>>>(kin, vin, kout, vout, pass, tiles, offs, lookback, st);
+  else
+    k_sort_pass<16><<<ntiles, kSortThreads, sort_smem<16>(), s>>>(kin, vin, kout, vout, pass, tiles, offs, lookback, st);
 }
 
 void launch_gather(const Particle* p, const uint32_t* perm, uint32_t n, Particle* staged, double4* pm, int sms,

@@ -11,9 +11,10 @@ void launch_bounds_domain(const Particle* p, const Tile* tiles, int ntiles, SysD
                           DevState* st, cudaStream_t s);
 void launch_keys(const Particle* p, const Tile* tiles, int ntiles, const SysDev* sys, int nsys, uint64_t* keys,
                  uint32_t* hist, uint32_t* offs, cudaStream_t s);
+// tiles: the sort's own tile table, tile_keys keys per tile (1024 or 4096)
 void launch_sort_pass(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout, int pass,
-                      const Tile* tiles, int ntiles, const uint32_t* offs, uint32_t* lookback, DevState* st,
-                      cudaStream_t s);
+                      const Tile* tiles, int ntiles, int tile_keys, const uint32_t* offs, uint32_t* lookback,
+                      DevState* st, cudaStream_t s);
 void launch_gather(const Particle* p, const uint32_t* perm, uint32_t n, Particle* staged, double4* pm, int sms,
                    cudaStream_t s);
 void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_t* keys, unsigned max_leaf,
