@@ -92,6 +92,7 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
     ap.add_argument("--serve-wall", type=float, default=None, help="serve: wall-clock window in seconds")
     ap.add_argument("--serve-duration", type=float, default=None, help="serve: length of the arrival stream")
+    ap.add_argument("--pipe-parts", type=int, default=4, help="ensemble e2e: contexts of the pipelined step")
     ap.add_argument("--serve-max-batch", type=int, default=None,
                     help="serve: also cap the particles one tick evaluates (latency-bounded batching)")
     return ap.parse_args()
@@ -515,9 +516,6 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     return out
 
 
-PIPE_PARTS = 4  # contexts of the pipelined end-to-end ensemble step
-
-
 def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
     from bhg import autotune
 
@@ -561,12 +559,12 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
 
         ems, ewall, _ = rig.time_steps(e2e_step, args.steps, 1)
         one_ctx_ms = max(ems, ewall)
-        # the same through bhg.pipeline: the systems in PIPE_PARTS contexts, each
-        # context's copies overlapping the others' evaluations (same bits)
+        # the same through bhg.pipeline: the systems in --pipe-parts contexts,
+        # each context's copies overlapping the others' evaluations (same bits)
         from bhg.pipeline import Pipeline
 
         host[:] = flat
-        pipe = Pipeline(counts, parts=PIPE_PARTS, device=rig.local)
+        pipe = Pipeline(counts, parts=args.pipe_parts, device=rig.local)
 
         def pipe_step():
             pipe.step(ptr, fp, leaf, w["group"], leaf, w["theta"], eps2, w["dt"], w["dt"])
@@ -576,7 +574,7 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
         ems = max(pms, pwall)  # wall clock: the contexts' streams are not the timing stream
         out["e2e"] = {"value": ps / (ems / 1000.0), "unit": "particle-steps/s", "h2d_bytes_per_step": n * 64,
                       "d2h_bytes_per_step": n * 64, "ms_per_step": ems / args.steps,
-                      "path": f"bhg.pipeline over {PIPE_PARTS} contexts: bhg_upload_systems (pinned host) + "
+                      "path": f"bhg.pipeline over {args.pipe_parts} contexts: bhg_upload_systems (pinned host) + "
                               "bhg_step_systems_async + bhg_download_async + bhg_sync",
                       "one_context": {"value": ps / (one_ctx_ms / 1000.0), "ms_per_step": one_ctx_ms / args.steps,
                                       "path": "bhg_upload_systems (pinned host) + bhg_step_systems + bhg_download"}}
