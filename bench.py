@@ -92,7 +92,7 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
     ap.add_argument("--serve-wall", type=float, default=None, help="serve: wall-clock window in seconds")
     ap.add_argument("--serve-duration", type=float, default=None, help="serve: length of the arrival stream")
-    ap.add_argument("--pipe-parts", type=int, default=4, help="ensemble e2e: contexts of the pipelined step")
+    ap.add_argument("--pipe-parts", type=int, default=8, help="ensemble e2e: contexts of the pipelined step")
     ap.add_argument("--serve-max-batch", type=int, default=None,
                     help="serve: also cap the particles one tick evaluates (latency-bounded batching)")
     return ap.parse_args()
