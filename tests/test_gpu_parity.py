@@ -147,6 +147,33 @@ def test_quadrupole_beats_monopole(gpu, oracle, precision):
     assert err[True] < err[False], err
 
 
+@pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-12), (bhg.PRECISION_SPLIT, 1e-5)])
+def test_deferral_overflow_falls_back(oracle, precision, tol):
+    """theta 0.2 on a uniform cube with one particle per leaf: some group walks
+    defer more nodes than a group's deferred list holds (up to ~1,200 against
+    512), so those groups' targets walk from the root, and walks outgrow the
+    stack and are redone one node at a time.  Lists and forces still match
+    the oracle's, in the two-pass and the one-pass schedule alike."""
+    parts = cube(8000, 5)
+    theta, eps2 = 0.2, 1e-6
+    dom, sk, perm, mp, t = _oracle_build(oracle, parts, 1)
+    tg = oracle.targets(t, 1, 64)
+    racc, counts = oracle.walk(t, tg, soa(mp), [Params(theta, eps2, 1.0, 1)] * len(tg))
+    accs = []
+    for budget in (0, 32 << 20):  # unlimited: two passes; 32 MB: no room for that buffer, one pass
+        with bhg.Context(device=0, hbm_budget=budget) as ctx:
+            ctx.upload(parts)
+            ctx.build_tree(1, 64)
+            ctx.compute_multipoles()
+            acc = ctx.walk_forces(bhg.Context.params(theta, eps2, 1.0, True, precision), 1)
+            st = ctx.stats()
+            assert (st["pp"], st["pc"]) == (int(counts[0]), int(counts[1])), "interaction counts differ"
+            assert rel_error(acc, racc) <= tol
+            accs.append((acc, st["kernels_per_eval"]))
+    assert accs[0][1] == accs[1][1] + 1  # the two schedules ran
+    assert accs[0][0].tobytes() == accs[1][0].tobytes()
+
+
 def test_no_softening_masks_self(gpu, oracle):
     # eps = 0: r^2 == 0 entries masked (accumulate_list Mask, grouped_ttg.h:117-123)
     parts = cube(3000, 9)
