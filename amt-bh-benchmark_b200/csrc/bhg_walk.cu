@@ -31,7 +31,7 @@
 // bounding-box centre (the subtraction in FP64), staged once per batch in
 // shared memory; interactions are FP32 FMA + rsqrt.approx.ftz, lanes laid out as
 // (target, source subset) (SplitEval below); FP32 partials go into FP64
-// sums after every batch.  The kick/drift of integrate_ttg.h:74-77 is
+// sums every 32 or more terms.  The kick/drift of integrate_ttg.h:74-77 is
 // applied in FP64 in the epilogue.
 #include "bhg_kernels.h"
 
@@ -105,9 +105,10 @@ __device__ __forceinline__ double far2(const double lo[3], const double hi[3], d
 // not one per lane group, and the lanes never exchange partial sums inside
 // a batch.  Each loop iteration evaluates two independent (source, target)
 // pairs: two sources for one target (kt = 1) or one source for two targets
-// (kt = 2).  FP32 partials are added into per-lane FP64 sums after every
-// batch; at the end of a walk the lane groups' FP64 sums are added in group
-// order (deterministic) into the targets' FP64 sums.
+// (kt = 2).  FP32 partials are added into per-lane FP64 sums once they hold
+// 32 or more terms (at most one batch's worth) and at the end of the walk;
+// then the lane groups' FP64 sums are added in group order (deterministic)
+// into the targets' FP64 sums.
 // rsqrt.approx.ftz.f32 (PTX ISA): the approximate reciprocal square root,
 // subnormal inputs and results flushed to zero.  The split evaluator's r^2 is
 // in units scaled to the system's size (at least eps^2 there, or masked when
@@ -121,6 +122,10 @@ __device__ __forceinline__ float rsqrt_ftz(float x) {
 template <bool QUAD, bool MASK>
 struct SplitEval {
   static constexpr int kCellBatch = 64, kPartBatch = 128;
+  // FP32 partials go into the FP64 sums once a lane has added kFlushTerms
+  // or more terms to them (so they never hold more than one 64-cell
+  // batch's worth), and at the end of the walk
+  static constexpr int kFlushTerms = 32;
   static constexpr int kCellDummy = kCellBatch;  // record index of the zero cell (written once)
   static constexpr int kPartDummy = kPartBatch;  // record index of the zero particle (written per batch)
   const WalkArgs& a;
@@ -140,6 +145,7 @@ struct SplitEval {
   float a0x, a0y, a0z, a1x, a1y, a1z;  // FP32 partials of the current batch
   double s0x, s0y, s0z, s1x, s1y, s1z;  // FP64 sums of this lane
   double (*acc)[3];  // the targets' FP64 sums (shared memory)
+  int pend;  // terms in this lane's FP32 partials since the last flush (an upper bound, warp-uniform)
 
   __device__ SplitEval(const WalkArgs& args, float4* stage_, int lane_) : a(args), stage(stage_), lane(lane_) {
     red = reinterpret_cast<double*>(stage_);
@@ -189,6 +195,7 @@ struct SplitEval {
     t1z = (float)(__dsub_rn(q1.z, cz) * scale);
     a0x = a0y = a0z = a1x = a1y = a1z = 0.f;
     s0x = s0y = s0z = s1x = s1y = s1z = 0.0;
+    pend = 0;
   }
 
   __device__ __forceinline__ void flush() {
@@ -265,7 +272,8 @@ struct SplitEval {
       cell_body(stage + 3 * s, t0x, t0y, t0z, a0x, a0y, a0z);
       cell_body(stage + 3 * sb, t1x, t1y, t1z, a1x, a1y, a1z);
     }
-    flush();
+    pend += (cnt + stride - 1) / stride;
+    if (pend >= kFlushTerms) flush(), pend = 0;
     __syncwarp();
   }
 
@@ -283,13 +291,15 @@ struct SplitEval {
       part_body(stage[s], t0x, t0y, t0z, a0x, a0y, a0z);
       part_body(stage[sb], t1x, t1y, t1z, a1x, a1y, a1z);
     }
-    flush();
+    pend += (cnt + stride - 1) / stride;
+    if (pend >= kFlushTerms) flush(), pend = 0;
     __syncwarp();
   }
 
   // After a walk: the lane groups' sums, added in group order into every
   // target's FP64 sum.
   __device__ void finish() {
+    if (pend) flush(), pend = 0;
     if (first < (1 << 30)) {
       double* r = red + 6 * lane;
       r[0] = s0x, r[1] = s0y, r[2] = s0z, r[3] = s1x, r[4] = s1y, r[5] = s1z;
