@@ -185,6 +185,7 @@ class Context:
             raise BhgError(r, "bhg_create failed (no GPU?)")
         self.h = h
         self.n = 0
+        self._snapbuf = None  # host buffer reused by snapshot_vtk
 
     def close(self):
         if self.h:
@@ -285,13 +286,28 @@ class Context:
         formatted on the GPU."""
         if handle is None:
             handle = int(self.system_ids()[0])
-        # one call, into a buffer of the largest possible size: three lines of
-        # at most 98 bytes per particle, plus the headers
-        cap = 98 * int(self.n) + 512
-        buf = np.empty(cap, np.uint8)
+        # one call, into a buffer of the largest possible size, kept for the
+        # next snapshot (its pages are then already mapped); the bytes object
+        # is a copy
+        cap = self.snapshot_vtk_bound()
+        if self._snapbuf is None or len(self._snapbuf) < cap:
+            self._snapbuf = np.zeros(cap, np.uint8)
+        n = self.snapshot_vtk_into(self._snapbuf, handle)
+        return self._snapbuf[:n].tobytes()
+
+    def snapshot_vtk_bound(self) -> int:
+        """Bytes that always hold a snapshot of this context's largest system:
+        three lines of at most 98 bytes per particle, plus the headers."""
+        return 98 * int(self.n) + 512
+
+    def snapshot_vtk_into(self, out: np.ndarray, handle=None) -> int:
+        """write_vtk's text of a system written into the caller's uint8 array
+        (pinned memory takes the fastest copy); returns the bytes written."""
+        if handle is None:
+            handle = int(self.system_ids()[0])
         n = C.c_size_t()
-        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, buf.ctypes.data_as(C.c_char_p), cap, C.byref(n)))
-        return buf[: n.value].tobytes()
+        self._ck(self.L.bhg_snapshot_vtk(self.h, handle, out.ctypes.data_as(C.c_char_p), out.nbytes, C.byref(n)))
+        return n.value
 
     def system_ids(self) -> np.ndarray:
         out = np.zeros(self.L.bhg_num_systems(self.h), np.uint64)
