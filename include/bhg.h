@@ -228,8 +228,8 @@ int bhg_step_systems(bhg_context* ctx, const bhg_force_params* fp, unsigned max_
  * stream and reports the enqueued evaluations: BHG_OK; BHG_EAGAIN when the
  * octree outgrew its node slots (they are grown: the state is as after the
  * last evaluation that ran, and the message says how many ran); or the
- * error that stopped them.  A blocking call after async ones reports them
- * first, as bhg_sync would. */
+ * error that stopped them.  A blocking step, or a call that changes the
+ * systems, after async ones reports them first, as bhg_sync would. */
 int bhg_step_systems_async(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
                            uint32_t target_size);
 int bhg_download_async(bhg_context* ctx, bh_particle64* out);
