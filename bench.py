@@ -739,9 +739,27 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
     if args.serve_max_batch is not None:
         w["max_batch_particles"] = args.serve_max_batch
     reqs = serve_stream(w)
+    # leaf (= target) size from the autotuner, on a sample of the stream's
+    # requests (their initial conditions from the same device generator) at
+    # theta 0.5, the accuracy gate's theta; theta itself is never tuned
+    from bhg import autotune
+
+    sample, tot = [], 0
+    for r in reqs[:64]:
+        if tot + r.n <= 8_000_000 and len(sample) < 16:
+            sample.append(r)
+            tot += r.n
+    with bhg.Context(device=rig.local) as c:
+        for r in sample:
+            c.add_generated(r.spheres(), r.seed, id0=0)
+        allp = c.download()
+    offs = np.cumsum([0] + [r.n for r in sample])
+    tuned = autotune.tune([allp[offs[i]:offs[i + 1]] for i in range(len(sample))], 0.5, w["eps"] ** 2, w["group"],
+                          bhg.PRECISION_SPLIT, device=rig.local)
+    leaf = tuned["max_leaf"]
     # warm-up: a few small requests through the same loop (kernels loaded,
     # occupancy queried)
-    warm = serve.Server(device=rig.local, hbm_budget=2e9, max_leaf=w["max_leaf"], group_size=w["group"])
+    warm = serve.Server(device=rig.local, hbm_budget=2e9, max_leaf=leaf, group_size=w["group"])
     warm.run([serve.Request(i, 0.0, "merger" if i % 2 else "plummer", 20000, 2, 0.5, 90 + i) for i in range(3)],
              realtime=False)
     warm.close()
@@ -750,7 +768,7 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
     def on_result(rid, parts):  # the finished state goes back to the host and is dropped
         delivered[0] += 1
 
-    srv = serve.Server(device=rig.local, hbm_budget=w["hbm_budget_gb"] * 1e9, max_leaf=w["max_leaf"],
+    srv = serve.Server(device=rig.local, hbm_budget=w["hbm_budget_gb"] * 1e9, max_leaf=leaf,
                        group_size=w["group"], on_result=on_result,
                        max_batch_particles=w.get("max_batch_particles"))
     srv.ctx.stats(reset=True)
@@ -798,9 +816,11 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
                 c.add_generated(pick.spheres(), pick.seed, id0=0)
                 parts = c.download()
                 fp = bhg.Context.params(0.5, pick.eps ** 2, 1.0, True, bhg.PRECISION_SPLIT)
-                out["force_error"] = force_error(c, parts, fp, w["max_leaf"], w["group"], w["max_leaf"], pick.eps ** 2)
-            out["force_error"]["system"] = f"request {pick.rid}: {pick.kind}, N={pick.n}, theta 0.5"
-    out["config_extra"] = {"mean_particles_per_tick": n_eval}
+                out["force_error"] = force_error(c, parts, fp, leaf, w["group"], leaf, pick.eps ** 2)
+            out["force_error"]["system"] = f"request {pick.rid}: {pick.kind}, N={pick.n}, theta 0.5, leaf {leaf}"
+    out["config_extra"] = {"mean_particles_per_tick": n_eval, "max_leaf_tuned": leaf}
+    out["autotune"] = {k: tuned[k] for k in ("max_leaf", "target_size", "rms_error", "err_budget", "table")}
+    out["autotune"]["sample"] = f"{len(sample)} of the stream's first 64 requests, {tot} particles, theta 0.5"
     return out
 
 
