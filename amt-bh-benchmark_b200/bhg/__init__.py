@@ -37,7 +37,7 @@ EXPORTED = (
     "bhg_step_systems_async", "bhg_download_async", "bhg_sync",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
     "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
-    "bhg_measure_fp32_peak",
+    "bhg_measure_fp32_peak", "bhg_selftest_wait",
 )
 
 
@@ -127,6 +127,7 @@ def lib() -> C.CDLL:
         "bhg_ic_plummer": ([vp, sz, f64, f64, vp, vp, u32, u64], u64),
         "bhg_write_csv": ([C.c_char_p, vp, sz], i32),
         "bhg_measure_fp32_peak": ([i32, C.POINTER(f64)], i32),
+        "bhg_selftest_wait": ([vp, i32, u32, C.POINTER(u32)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -419,6 +420,16 @@ class Context:
         self._ck(self.L.bhg_direct_sum(self.h, system, _p(idx), len(idx), eps2, G, _p(out)))
         return out
 
+    def selftest_wait(self, publish_first: bool, spin_limit: int):
+        """bhg_selftest_wait: (status code, prefix) of the bounded look-back
+        wait run on a prepared array whose first tile publishes or never does."""
+        pre = C.c_uint32()
+        r = self.L.bhg_selftest_wait(self.h, 1 if publish_first else 0, spin_limit, C.byref(pre))
+        return r, pre.value
+
+    def last_error(self) -> str:
+        return (self.L.bhg_last_error(self.h) or b"").decode(errors="replace")
+
     def energy(self, G=1.0, system=0):
         k, p = C.c_double(), C.c_double()
         self._ck(self.L.bhg_energy(self.h, system, G, C.byref(k), C.byref(p)))
@@ -443,7 +454,14 @@ def ensemble(nsys=512, seed=3, nmin=1024, nmax=262144):
     """Independent Plummer systems (M = a = 1 each) with N log-uniform in
     [nmin, nmax]: N_s = round(exp(U(ln nmin, ln nmax))) and per-system seeds,
     both from numpy's PCG64 stream `seed`.  Returns a list of particle arrays."""
+    ns, seeds = ensemble_specs(nsys, seed, nmin, nmax)
+    return [plummer(int(n), int(sd))[0] for n, sd in zip(ns, seeds)]
+
+
+def ensemble_specs(nsys=512, seed=3, nmin=1024, nmax=262144):
+    """The sizes and generator seeds of :func:`ensemble`'s systems (numpy only:
+    loads nothing of the GPU library)."""
     rng = np.random.default_rng(seed)
     ns = np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsys))).astype(np.int64)
     seeds = rng.integers(1, 2**63 - 1, nsys)
-    return [plummer(int(n), int(sd))[0] for n, sd in zip(ns, seeds)]
+    return ns, seeds

@@ -615,11 +615,8 @@ int set_force_params(bhg_context* c, const bhg_force_params* fp, double kick, do
     return fail(c, BHG_EINVAL, "theta and eps2 must be >= 0, G finite");
   if (fp->precision != BHG_PRECISION_SPLIT && fp->precision != BHG_PRECISION_FP64)
     return fail(c, BHG_EINVAL, "unknown precision");
-  const int newq = fp->use_quadrupole ? 1 : 0;
-  const bool newmask = !(fp->eps2 > 0.0);
-  c->quad = newq;
+  c->quad = fp->use_quadrupole ? 1 : 0;
   c->precision = fp->precision;
-  c->mask = newmask;
   for (auto& p : c->prm_host) {
     if (!keep_per_system) {
       p.theta2 = fp->theta * fp->theta;
@@ -629,6 +626,17 @@ int set_force_params(bhg_context* c, const bhg_force_params* fp, double kick, do
     }
     p.G = fp->G;
   }
+  // The r^2 = 0 self term is masked (accumulate_list, grouped_ttg.h:117-123)
+  // when a walked system has no softening.  With per-system parameters the
+  // systems' own eps2 decide, not fp->eps2: one unsoftened system among
+  // softened ones needs the masked kernel (its self terms would be
+  // rsqrt(0) = inf times 0 otherwise).
+  bool mask = !(fp->eps2 > 0.0);
+  if (keep_per_system) {
+    mask = false;
+    for (const auto& p : c->prm_host) mask = mask || !(p.eps2 > 0.0);
+  }
+  c->mask = mask;
   return BHG_OK;
 }
 
@@ -755,18 +763,22 @@ static int add_system_impl(bhg_context* c, size_t n, uint64_t* id, F fill) {
   const size_t old = c->n;
   c->counts.push_back(n);
   c->ids.push_back(c->next_id);
-  int r = relayout(c);
-  if (r) {
+  const uint64_t handle = c->next_id;
+  auto roll_back = [&](int code) {
     const std::string why = c->err;
     c->counts.pop_back();
     c->ids.pop_back();
     c->n = old;
     relayout(c);  // a failure here leaves capacities at 0, which the next call repairs
-    return fail(c, r, why);
-  }
-  if ((r = fill(c->part + old))) return r;
-  if (id) *id = c->next_id;
+    return fail(c, code, why);
+  };
+  int r = relayout(c);
+  if (r) return roll_back(r);
+  // the handle is spent before the fill: a failed fill can never leave two
+  // resident systems with one handle
   ++c->next_id;
+  if ((r = fill(c->part + old))) return roll_back(r);
+  if (id) *id = handle;
   return BHG_OK;
 }
 
@@ -1524,6 +1536,38 @@ int bhg_energy(bhg_context* c, int sys, double G, double* kinetic, double* poten
   if (kinetic) *kinetic = ek;
   if (potential) *potential = ep;
   return BHG_OK;
+}
+
+int bhg_selftest_wait(bhg_context* c, int publish_first, uint32_t spin_limit, uint32_t* prefix) {
+  if (!c) return BHG_EINVAL;
+  if (spin_limit == 0 || spin_limit > (1u << 20))
+    return fail(c, BHG_EINVAL, "spin_limit must be in 1 .. 2^20 (a short wait)");
+  cudaSetDevice(c->device);
+  int r = read_state(c);  // finish what is queued; its own errors come first
+  if (r || (r = finish_async(c))) return r;
+  constexpr uint32_t kTiles = 8;
+  uint32_t* words = nullptr;
+  if ((r = dev_alloc(c, reinterpret_cast<void**>(&words), (kTiles + 1) * sizeof(uint32_t)))) return r;
+  // tiles 1..7 have published an aggregate of 1 each; tile 0 publishes an
+  // inclusive prefix of 1, or nothing at all
+  uint32_t h[kTiles + 1] = {};
+  for (uint32_t t = 1; t < kTiles; ++t) h[t] = kFlagAgg | 1u;
+  h[0] = publish_first ? (kFlagPre | 1u) : 0u;
+  cudaError_t e = cudaMemcpyAsync(words, h, sizeof h, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    launch_wait_probe(words, kTiles, (int)spin_limit, c->st, words + kTiles, c->stream);
+    e = cudaGetLastError();
+  }
+  uint32_t got = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&got, words + kTiles, sizeof got, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  dev_free(c, words);
+  if (e != cudaSuccess) return fail(c, BHG_ECUDA, std::string("selftest_wait: ") + cudaGetErrorString(e));
+  if (prefix) *prefix = got;
+  if ((r = read_state(c))) return r;
+  r = check_status(c);  // a wait that gave up: BHG_EDEVICE, as from a real sort or scan
+  clear_status(c);
+  return r;
 }
 
 int bhg_measure_fp32_peak(int device, double* tflops) {

@@ -47,9 +47,12 @@ __device__ inline uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t* t
 }
 
 // Waits (bounded) for the look-back word of tile t and sums predecessors
-// until an inclusive prefix is found.  first: the chain's first tile.
+// until an inclusive prefix is found.  first: the chain's first tile.  A
+// predecessor that has not published after `limit` polls ends the wait: the
+// status bit kStSpinLimit is set and the (partial) sum returned, so the
+// kernel finishes and the host reports BHG_EDEVICE instead of hanging.
 __device__ inline uint32_t look_back(const uint32_t* words, uint32_t t, uint32_t first, uint32_t stride,
-                                     DevState* st) {
+                                     DevState* st, int limit = kSpinLimit) {
   uint32_t excl = 0;
   while (t > first) {
     --t;
@@ -57,7 +60,7 @@ __device__ inline uint32_t look_back(const uint32_t* words, uint32_t t, uint32_t
     int spins = 0;
     do {
       w = ld_volatile(&words[(size_t)t * stride]);
-    } while ((w >> 30) == 0u && ++spins < kSpinLimit);
+    } while ((w >> 30) == 0u && ++spins < limit);
     if ((w >> 30) == 0u) {
       atomicOr(&st->status, kStSpinLimit);
       return excl;
@@ -66,6 +69,17 @@ __device__ inline uint32_t look_back(const uint32_t* words, uint32_t t, uint32_t
     if ((w & kFlagPre) == kFlagPre) return excl;
   }
   return excl;
+}
+
+// The wait above on a caller-prepared word array (bhg_selftest_wait): one
+// thread looks back from tile `tile` to tile 0 with the given poll limit and
+// writes the exclusive prefix it found.
+__global__ void k_wait_probe(const uint32_t* words, uint32_t tile, int limit, DevState* st, uint32_t* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[0] = look_back(words, tile, 0, 1, st, limit);
+}
+
+void launch_wait_probe(const uint32_t* words, uint32_t tile, int limit, DevState* st, uint32_t* out, cudaStream_t s) {
+  k_wait_probe<<<1, 32, 0, s>>>(words, tile, limit, st, out);
 }
 
 // ---------------------------------------------------------------------------

@@ -7,6 +7,9 @@
 namespace bhg {
 
 void set_build_attributes();
+// The sort/scan kernels' bounded look-back wait on a prepared array of tile
+// words (a self-test of the give-up path): exclusive prefix of `tile` to out[0].
+void launch_wait_probe(const uint32_t* words, uint32_t tile, int limit, DevState* st, uint32_t* out, cudaStream_t s);
 void launch_bounds_domain(const Particle* p, const Tile* tiles, int ntiles, SysDev* sys, int nsys, double* partial,
                           DevState* st, cudaStream_t s);
 void launch_keys(const Particle* p, const Tile* tiles, int ntiles, const SysDev* sys, int nsys, uint64_t* keys,
@@ -77,7 +80,8 @@ void launch_integrate(Particle* p, const double* accel, uint32_t n, const SysDev
 void launch_eval_done(DevState* st, cudaStream_t s);
 void launch_direct(const double4* pm, uint32_t begin, uint32_t n, const uint32_t* idx, uint32_t ns, double eps2,
                    double G, double* out, cudaStream_t s);
-void launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int sms, cudaStream_t s);
+cudaError_t launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int sms,
+                          cudaStream_t s);
 double measure_fp32_peak(int device);
 // Particle text (bhg_csv.cu).  Ingest: newline count per 16 KB tile and the
 // scan of the tile counts (total newlines to *total), then the line starts

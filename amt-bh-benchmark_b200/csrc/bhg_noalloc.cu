@@ -11,6 +11,8 @@
 #include "bhg.h"
 #include "bhg_kernels.h"
 
+#include <cuda.h>
+
 #include <mutex>
 
 namespace {
@@ -25,25 +27,48 @@ constexpr size_t kNoAllocMaxParticles = (size_t)kNoAllocMaxBlocks * kNoAllocThre
 static __device__ __align__(256) double g_energy_partials[2 * kNoAllocMaxBlocks];
 
 // Host code may not hand the symbol itself to a kernel (on the host it names
-// a stand-in, not device memory); this is its device address per device,
-// looked up once with that device current.
-constexpr int kMaxDevices = 64;
+// a stand-in, not device memory); this is its device address, looked up with
+// the device current.  The address belongs to the CUDA context the library's
+// module was loaded into: after cudaDeviceReset the device gets a new primary
+// context where the array may sit elsewhere.  So the lookups are cached per
+// context (the driver's cuCtxGetCurrent, reached through the runtime's entry
+// point table: no link against libcuda), and a new context looks it up again.
+constexpr int kCacheSlots = 64;
 std::mutex g_setup_mutex;
-double* g_partials_ptr[kMaxDevices] = {};
+struct Slot {
+  CUcontext ctx;
+  double* ptr;
+};
+Slot g_slots[kCacheSlots] = {};
+int g_next_slot = 0;
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
 
-int partials_for_current_device(double** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BHG_ECUDA;
+int partials_for_current_context(double** out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_partials_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_energy_partials) != cudaSuccess) {
-      cudaGetLastError();
+  if (!g_ctx_get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
       return BHG_ECUDA;
-    }
-    g_partials_ptr[dev] = static_cast<double*>(p);
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
   }
-  *out = g_partials_ptr[dev];
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return BHG_ECUDA;
+  for (const Slot& s : g_slots)
+    if (ctx && s.ctx == ctx && s.ptr) {
+      *out = s.ptr;
+      return BHG_OK;
+    }
+  // the lookup also makes the current device's primary context current on
+  // this thread when none was
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_energy_partials) != cudaSuccess) return BHG_ECUDA;
+  if (!ctx && (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx)) return BHG_ECUDA;
+  g_slots[g_next_slot] = Slot{ctx, static_cast<double*>(p)};
+  g_next_slot = (g_next_slot + 1) % kCacheSlots;
+  *out = static_cast<double*>(p);
   return BHG_OK;
 }
 
@@ -66,13 +91,18 @@ extern "C" int bhg_energy_noalloc(const bh_particle64* particles, size_t n, doub
   if (!particles || !result || n == 0) return BHG_EINVAL;
   if (n > kNoAllocMaxParticles) return BHG_EINVAL;  // more than the fixed partial-sum array can hold
   double* partials = nullptr;
-  int r = partials_for_current_device(&partials);
+  int r = partials_for_current_context(&partials);
   if (r) return r;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int nblocks = (int)((n + kNoAllocThreads - 1) / kNoAllocThreads);
+  int nblocks = (int)((n + kNoAllocThreads - 1) / kNoAllocThreads);
   // every partial this call reads is written by this call's k_energy first,
-  // so the array needs no clearing between calls
-  bhg::launch_energy(reinterpret_cast<const bhg::Particle*>(particles), 0u, (uint32_t)n, G, partials, 0, s);
-  k_energy_total<<<1, 1, 0, s>>>(partials, nblocks, result);
-  return cudaGetLastError() == cudaSuccess ? BHG_OK : BHG_ECUDA;
+  // so the array needs no clearing between calls.  Each launch reports its
+  // own error: an unrelated error left on the thread by an earlier call is
+  // neither returned as this call's nor cleared.
+  if (bhg::launch_energy(reinterpret_cast<const bhg::Particle*>(particles), 0u, (uint32_t)n, G, partials, 0, s) !=
+      cudaSuccess)
+    return BHG_ECUDA;
+  void* args[] = {(void*)&partials, (void*)&nblocks, (void*)&result};
+  if (cudaLaunchKernel((const void*)k_energy_total, dim3(1), dim3(1), args, 0, s) != cudaSuccess) return BHG_ECUDA;
+  return BHG_OK;
 }

@@ -1068,8 +1068,11 @@ __global__ void __launch_bounds__(kEnThreads) k_energy(const Particle* __restric
   }
 }
 
-void launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int, cudaStream_t s) {
-  k_energy<<<(n + kEnThreads - 1) / kEnThreads, kEnThreads, 0, s>>>(p, begin, n, G, out2);
+// Returns this launch's own error (cudaLaunchKernel reports it directly, so
+// an unrelated earlier error left on the thread is neither returned nor cleared).
+cudaError_t launch_energy(const Particle* p, uint32_t begin, uint32_t n, double G, double* out2, int, cudaStream_t s) {
+  void* args[] = {(void*)&p, (void*)&begin, (void*)&n, (void*)&G, (void*)&out2};
+  return cudaLaunchKernel((const void*)k_energy, dim3((n + kEnThreads - 1) / kEnThreads), dim3(kEnThreads), args, 0, s);
 }
 
 // ---------------------------------------------------------------------------

@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="ensemble: skip the one-at-a-time FP64 path")
+    ap.add_argument("--no-north-star", action="store_true",
+                    help="plummer-4m: skip the ensemble and serving gates run after the main measurement")
     ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
     ap.add_argument("--serve-wall", type=float, default=None, help="serve: wall-clock window in seconds")
     ap.add_argument("--serve-duration", type=float, default=None, help="serve: length of the arrival stream")
@@ -168,6 +170,42 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---------------------------------------------------------------------------- workload description
+
+L2_NOTE = "inputs larger than L2 (particle state, Morton copy and tree exceed 126 MB)"
+
+
+def workload_particles(w):
+    """Total particles of a workload (numpy only: loads nothing of the GPU library)."""
+    if w["kind"] in ("single", "csv", "merger"):
+        return int(w["n"])
+    if w["kind"] == "ensemble":
+        import bhg
+
+        return int(np.sum(bhg.ensemble_specs(w["nsys"], w["seed"])[0]))
+    return None
+
+
+def workload_config(name, w, world):
+    """The `config` object of both arms' JSON lines (one function, so the two
+    lines describe the workload identically)."""
+    cfg = {"workload": name, **{k: (list(v) if isinstance(v, tuple) else v) for k, v in w.items() if k != "kind"}}
+    cfg["n_particles"] = workload_particles(w)
+    cfg["parallelism"] = f"replicas x{world}"
+    cfg["l2"] = L2_NOTE
+    return cfg
+
+
+def workload_spheres(w, n=None):
+    """The workload's initial conditions as generator spheres (same sampling as
+    bhg.plummer / bhg.merger): a list of dicts n, a, mass, centre, bulk."""
+    n = n or w["n"]
+    if w["kind"] == "merger":
+        return [dict(n=n // 2, a=1.0, mass=1.0, centre=(-5.0, 0.0, 0.0), bulk=(0.15, 0.0, 0.0)),
+                dict(n=n // 2, a=0.5, mass=1.0, centre=(5.0, 0.0, 0.0), bulk=(-0.15, 0.0, 0.0))]
+    return [dict(n=n, a=1.0, mass=1.0)]
+
+
 # ---------------------------------------------------------------------------- CPU reference
 
 def ref_binary():
@@ -182,83 +220,69 @@ def ref_binary():
     return v3 if os.path.exists(v3) else None
 
 
-def run_ref(parts, w, evals, leaf=None):
-    """Times `evals` evaluations of the reference schedule; returns (eval ms list, threads)."""
+def run_ref(spheres, seed, w, warmup_evals=0, timed_evals=None, leaf=None, theta=None):
+    """The reference's schedule (oracle/_ref/ref_bench, its own process) on
+    Plummer spheres it generates from `seed`: `warmup_evals` untimed
+    evaluations, then `timed_evals` timed ones (default: one whole schedule),
+    schedules back to back.  Returns (timed eval ms list, threads)."""
     exe = ref_binary()
     if exe is None:
         raise FileNotFoundError("oracle/_ref/ref_bench is not built")
-    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
-        parts.tofile(f)
-        path = f.name
     leaf = leaf or w["max_leaf"]
-    try:
-        cmd = [exe, "--particles", path, "--steps", str(w["steps"]), "--evals", str(evals), "--dt", repr(w["dt"]),
-               "--theta", repr(w["theta"]), "--eps", repr(w["eps"]), "--max-leaf", str(leaf),
-               "--target-size", str(w["target"] if leaf == w["max_leaf"] else leaf),
-               "--group-size", str(w["group"])]
-        out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
-    finally:
-        os.unlink(path)
+    cmd = [exe, "--seed", str(int(seed))]
+    for sp in spheres:
+        c, b = sp.get("centre", (0.0, 0.0, 0.0)), sp.get("bulk", (0.0, 0.0, 0.0))
+        cmd += ["--sphere", ",".join(repr(float(x)) for x in (sp["n"], sp.get("a", 1.0), sp.get("mass", 1.0), *c, *b))]
+    cmd += ["--steps", str(w["steps"]), "--dt", repr(w["dt"]), "--theta", repr(theta if theta is not None else w["theta"]),
+            "--eps", repr(w["eps"]), "--max-leaf", str(leaf),
+            "--target-size", str(w["target"] if leaf == w["max_leaf"] else leaf), "--group-size", str(w["group"]),
+            "--warmup-evals", str(warmup_evals), "--timed-evals", str(timed_evals if timed_evals else w["steps"] + 1)]
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
     rec = json.loads(out.strip().splitlines()[-1])
     return rec["eval_ms"], rec["threads"]
 
 
-def cpu_sample(w, budget_s=20.0):
-    """A bounded sample of a single-system workload on the reference: the full
-    system if one evaluation fits the budget, else the largest power-of-two
-    system of the same kind and parameters that does.  Returns (n, eval ms, threads)."""
-    import bhg
-
-    def gen(n):
-        return bhg.merger(n // 2, w["seed"]) if w["kind"] == "merger" else bhg.plummer(n, w["seed"])[0]
-
+def ref_sample_n(w, evals, budget_s):
+    """The largest system (the full one, else a power of two of the same kind
+    and parameters) whose `evals` reference evaluations fit about budget_s,
+    from a timed probe at 65,536 particles (the cost per particle grows
+    slowly with N)."""
     n_probe = min(w["n"], 65536)
-    ms, threads = run_ref(gen(n_probe), w, 2)
-    per = ms[-1] / n_probe  # ms per particle per evaluation
+    ms, _ = run_ref(workload_spheres(w, n_probe), w["seed"], w, 1, 1)
+    per = ms[-1] / n_probe / 1000.0  # s per particle per evaluation
+    if per * w["n"] * 1.25 * evals <= budget_s:
+        return w["n"]
     n = n_probe
-    while n * 2 <= w["n"] and per * (n * 2) * 1.15 * 2 / 1000.0 < budget_s:
+    while n * 2 < w["n"] and per * 1.1 * (n * 2) * 1.25 * evals <= budget_s:
         n *= 2
-        per *= 1.1  # the walk cost per particle grows with log N
-    if n != n_probe:
-        ms, threads = run_ref(gen(n), w, 2)
-    return n, ms, threads
+        per *= 1.1
+    return n
 
 
 def cpu_rate(n, eval_ms, w):
     """particle-steps/s of the schedule (steps advances per steps+1 evaluations)."""
-    t = float(np.mean(eval_ms[1:] if len(eval_ms) > 1 else eval_ms)) / 1000.0
+    t = float(np.mean(eval_ms)) / 1000.0
     return n * w["steps"] / ((w["steps"] + 1) * t)
 
 
-def cpu_ensemble_sample(w, systems, budget_particles=600000):
+def cpu_ensemble_sample(w, budget_particles=600000):
     """The reference on a seeded random subset of the ensemble's systems (one
     evaluation each after one untimed): rate = sum N / sum eval time."""
-    order = np.random.default_rng(99).permutation(len(systems))
+    import bhg
+
+    ns, seeds = bhg.ensemble_specs(w["nsys"], w["seed"])
+    order = np.random.default_rng(99).permutation(len(ns))
     n_tot, t_tot, used, threads = 0, 0.0, 0, None
     for s in order:
-        ms, threads = run_ref(systems[s], w, 2)
-        n_tot += len(systems[s])
+        ms, threads = run_ref([dict(n=int(ns[s]), a=1.0, mass=1.0)], int(seeds[s]), w, 1, 1)
+        n_tot += int(ns[s])
         t_tot += ms[-1] / 1000.0
         used += 1
         if n_tot >= budget_particles:
             break
-    sample = (f"{used} of {len(systems)} systems ({n_tot} particles), one timed (dt, dt) evaluation each after "
+    sample = (f"{used} of {len(ns)} systems ({n_tot} particles), one timed (dt, dt) evaluation each after "
               f"one untimed, through bh::step_particles; rate = sum N / sum eval time")
     return n_tot / t_tot, threads, sample
-
-
-def serve_request_particles(req):
-    """A served request's initial conditions drawn by the host generator (the
-    distribution of the device generator)."""
-    import bhg
-
-    seed = req.seed % (1 << 63)
-    if req.kind == "plummer":
-        return bhg.plummer(req.n, seed)[0]
-    sp = req.spheres()
-    p1, nxt = bhg.plummer(sp[0]["n"], seed, a=sp[0]["a"], centre=sp[0]["centre"], bulk=sp[0]["bulk"])
-    p2, _ = bhg.plummer(sp[1]["n"], nxt, a=sp[1]["a"], centre=sp[1]["centre"], bulk=sp[1]["bulk"], id0=sp[0]["n"])
-    return np.concatenate([p1, p2])
 
 
 def serve_stream(w):
@@ -271,12 +295,14 @@ def serve_stream(w):
 def cpu_serve_sample(w, budget_particles=600000):
     """The reference on the stream's first requests, one at a time (it serves
     one simulation per process): one timed (dt, dt) evaluation per request
-    after one untimed, at the request's own theta.  Returns (rate, threads, sample)."""
+    after one untimed, at the request's own theta, its initial conditions
+    drawn by the host generator from the request's seed (the distribution of
+    the device generator).  Returns (rate, threads, sample)."""
     n_tot, t_tot, used, threads = 0, 0.0, 0, None
     for r in serve_stream(w):
         if n_tot + r.n > budget_particles:
             continue
-        ms, threads = run_ref(serve_request_particles(r), dict(w, theta=r.theta, steps=r.steps), 2)
+        ms, threads = run_ref(r.spheres(), r.seed % (1 << 63), dict(w, steps=r.steps), 1, 1, theta=r.theta)
         n_tot += r.n
         t_tot += ms[-1] / 1000.0
         used += 1
@@ -318,12 +344,22 @@ def cpu_csv_sample(w):
 
 
 def reference_arm(args, w):
+    """The reference's own CPU implementation of the path (oracle/_ref/ref_bench:
+    its unmodified sources, all host cores) on the same workload, metric and
+    config.  Single systems: one bench step = one force evaluation of the
+    workload's leapfrog schedule (schedules run back to back), --warmup
+    untimed evaluations, then exactly --steps timed ones, on the full system
+    when that fits a few minutes (else the largest power-of-two system of the
+    same kind); value = N * steps / ((steps + 1) * mean evaluation time), the
+    particle-steps/s of whole schedules.  The process loads nothing of the GPU
+    library: ref_bench draws the initial conditions itself (same generator)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    import bhg
-
     unit = "particle-steps/s" if w["kind"] != "csv" else "particles/s"
+    step_note = None
+    steps_done, warm_done = args.steps, args.warmup
     if w["kind"] == "csv":
         value, threads, sample = cpu_csv_sample(w)
         ms_step = w["n"] / value * 1000.0
@@ -331,30 +367,29 @@ def reference_arm(args, w):
         value, threads, sample = cpu_serve_sample(w)
         ms_step = None
     elif w["kind"] == "ensemble":
-        systems = make_particles(w)
-        value, threads, sample = cpu_ensemble_sample(w, systems)
-        n = sum(len(p) for p in systems)
-        ms_step = n / value * 1000.0
+        value, threads, sample = cpu_ensemble_sample(w)
+        ms_step = workload_particles(w) / value * 1000.0
     else:
-        n, _, _ = cpu_sample(w)
-        parts = bhg.merger(n // 2, w["seed"]) if w["kind"] == "merger" else bhg.plummer(n, w["seed"])[0]
-        ms, threads = run_ref(parts, w, args.warmup + args.steps)
-        timed = ms[args.warmup:]
-        value = cpu_rate(n, [0.0] + timed, w)
-        ms_step = float(np.mean(timed))
+        n = ref_sample_n(w, args.warmup + args.steps, budget_s=150.0)
+        ms, threads = run_ref(workload_spheres(w, n), w["seed"], w, args.warmup, args.steps)
+        value = cpu_rate(n, ms, w)
+        ms_step = float(np.mean(ms))
+        step_note = (f"one bench step = one force evaluation of the {w['steps']}-step schedule "
+                     f"({w['steps'] + 1} evaluations per schedule, run back to back); "
+                     f"ms per schedule = {ms_step * (w['steps'] + 1):.1f}")
         sample = (f"{'full system' if n == w['n'] else f'N={n}, same generator and parameters'}: "
-                  f"{len(timed)} force evaluations of the reference schedule through bh::step_particles, "
+                  f"{args.warmup} untimed then {len(ms)} timed force evaluations through bh::step_particles; "
                   f"rate = N*{w['steps']}/({w['steps'] + 1}*mean eval time)")
     line = {
         "impl": "reference", "metric": METRIC if w["kind"] != "csv" else "csv-ingest particles/s", "value": value,
-        "unit": unit, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "unit": unit, "n_gpus": args.gpus, "steps": steps_done, "warmup": warm_done, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, **{k: v for k, v in w.items() if k != "kind"}, "threads": threads},
-        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "reference",
-                         "sample": sample},
+        "config": workload_config(args.workload, w, world),
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if step_note:
+        line["step"] = step_note
     print(json.dumps(line), flush=True)
     return 0
 
@@ -459,10 +494,14 @@ def force_error(ctx, parts, fp, leaf, group, target, eps2, nsample=4096):
 
 
 def cpu_single(w):
+    """The CPU-baseline leg of the GPU arm's line: the reference on the
+    workload's system (bounded to ~20 s: the full system, else a smaller one
+    of the same kind), one timed evaluation after one untimed."""
     try:
-        ns, ems_cpu, threads = cpu_sample(w)
-        return {"value": cpu_rate(ns, ems_cpu, w), "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-                "sample": (f"{'full system' if ns == w['n'] else f'N={ns}, same generator and parameters'}: "
+        n = ref_sample_n(w, 2, budget_s=20.0)
+        ms, threads = run_ref(workload_spheres(w, n), w["seed"], w, 1, 1)
+        return {"value": cpu_rate(n, ms, w), "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                "sample": (f"{'full system' if n == w['n'] else f'N={n}, same generator and parameters'}: "
                            f"1 timed force evaluation (after 1 untimed) of the reference schedule through "
                            f"bh::step_particles; rate = N*{w['steps']}/({w['steps'] + 1}*eval time)")}
     except (OSError, subprocess.CalledProcessError) as e:
@@ -516,8 +555,14 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     return out
 
 
-def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
+def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
+    """quick: the north-star check inside the default run - fewer timed
+    steps, no pipelined end-to-end leg, no CPU baseline."""
     from bhg import autotune
+
+    if quick:
+        args = argparse.Namespace(**vars(args))
+        args.steps, args.warmup, args.no_e2e, args.no_cpu_baseline, args.no_plain = 3, 2, True, True, False
 
     systems = make_particles(w, rig.rank)
     ns = len(systems)
@@ -616,7 +661,7 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks):
 
     if rig.rank == 0 and not args.no_cpu_baseline:
         try:
-            v, threads, sample = cpu_ensemble_sample(w, systems)
+            v, threads, sample = cpu_ensemble_sample(w)
             out["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
                                    "sample": sample}
         except (OSError, subprocess.CalledProcessError) as e:
@@ -725,10 +770,17 @@ def bench_csv(args, w, rig, bhg, peaks):
     return out
 
 
-def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
+def bench_serve(args, w, rig, bhg, fp32_peak, peaks, quick=False):
     """The request loop in real time over the Poisson stream, for a bounded
-    wall window; value = particle-steps completed / wall time."""
+    wall window; value = particle-steps completed / wall time.  quick: the
+    north-star check inside the default run - a 30 s window, no CPU baseline."""
     from bhg import serve
+
+    w = dict(w)
+    if quick:
+        args = argparse.Namespace(**vars(args))
+        args.no_cpu_baseline = True
+        args.serve_wall = args.serve_wall or 30.0
 
     if args.serve_budget_gb is not None:
         w["hbm_budget_gb"] = args.serve_budget_gb
@@ -824,6 +876,37 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks):
     return out
 
 
+def north_star_block(args, rig, bhg, fp32_peak, peaks):
+    """The two throughput gates of the batched and served paths, measured in
+    the default run (each with its own clock record):
+
+    * ensemble-512: the 512-system ensemble in one segmented key space,
+      split precision, tuned leaf, against the plain FP64 path stepping the
+      systems one at a time (gate: >= 4x, rms force error <= 1e-3);
+    * serve-200rps: the continuous-batching server on the Poisson request
+      stream for a 30 s window (p50/p99 per-step latency, aggregate
+      particle-steps/s)."""
+    out = {}
+    e = bench_ensemble(args, WORKLOADS["ensemble-512"], rig, bhg, fp32_peak, peaks, quick=True)
+    if rig.rank == 0:
+        out["ensemble_512"] = {
+            "value": e["value"], "unit": "particle-steps/s", "ms_per_step": e["ms_per_step"], "steps": 3,
+            "warmup": 2, "plain_fp64_one_at_a_time": e.get("plain_fp64_one_at_a_time"),
+            "speedup_vs_plain": e.get("speedup_vs_plain"), "gate_speedup": 4.0,
+            "force_error": e.get("force_error"), "clocks": e.get("clocks"),
+            "walk_roofline_frac": e["roofline"]["frac"], "autotune": e.get("autotune"),
+            "details": e.get("config_extra")}
+    sv = bench_serve(args, WORKLOADS["serve-200rps"], rig, bhg, fp32_peak, peaks, quick=True)
+    if rig.rank == 0:
+        out["serve_200rps"] = {
+            "value": sv["value"], "unit": "particle-steps/s", "latency_ms": sv.get("latency_ms"),
+            "window_s": sv["serving"].get("wall_s"), "completed": sv["serving"].get("completed"),
+            "admitted": sv["serving"].get("admitted"), "force_error": sv.get("force_error"),
+            "clocks": sv.get("clocks"), "walk_roofline_frac": sv["roofline"]["frac"],
+            "details": sv.get("config_extra")}
+    return out
+
+
 def main():
     args = parse()
     w = WORKLOADS[args.workload]
@@ -846,17 +929,18 @@ def main():
     else:
         res = bench_single(args, w, rig, bhg, fp32_peak, peaks)
         dtype = "f32+f64" if args.precision == "split" else "f64"
+    if w["kind"] == "single" and args.workload == "plummer-4m" and not args.no_north_star:
+        res["north_star"] = north_star_block(args, rig, bhg, fp32_peak, peaks)
     if rig.rank == 0:
-        cfg = {"workload": args.workload, **{k: v for k, v in w.items() if k != "kind"},
-               **res.pop("config_extra"),
-               "precision": args.precision if w["kind"] in ("single", "merger") else "split",
-               "parallelism": f"replicas x{rig.world}",
-               "l2": "inputs larger than L2 (particle state, Morton copy and tree exceed 126 MB)"}
+        cfg = workload_config(args.workload, w, rig.world)
         metric, unit = (METRIC, "particle-steps/s") if w["kind"] != "csv" else ("csv-ingest particles/s", "particles/s")
+        details = res.pop("config_extra")
         line = {"metric": metric, "value": res.pop("value"), "unit": unit, "n_gpus": rig.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
-                "data": "synthetic", "config": cfg, **res}
+                "data": "synthetic", "config": cfg,
+                "precision": args.precision if w["kind"] in ("single", "merger") else "split", "details": details,
+                **res}
         print(json.dumps(line), flush=True)
     rig.rep.close()
     return 0

@@ -216,7 +216,9 @@ int bhg_step(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, ui
              uint32_t target_size, double kick_dt, double drift_dt);
 /* One evaluation of every system with the per-system theta, eps2, kick_dt
  * and drift_dt last given to bhg_set_system_params (fp supplies G, the
- * quadrupole switch and the precision). */
+ * quadrupole switch and the precision; fp->eps2 is not used: a system with
+ * eps2 0 gets the reference's r^2 = 0 self-term mask whatever the others
+ * have). */
 int bhg_step_systems(bhg_context* ctx, const bhg_force_params* fp, unsigned max_leaf, uint32_t group_size,
                      uint32_t target_size);
 /* Asynchronous forms, for overlapping one context's copies with another's
@@ -280,11 +282,27 @@ int bhg_energy(bhg_context* ctx, int sys, double G, double* kinetic, double* pot
  * potential).  Allocates nothing: the per-block partial sums live in a fixed
  * 16 KB array in the library's device memory, so n is at most 262,144 (larger
  * n returns BHG_EINVAL).  Asynchronous on `stream` (a cudaStream_t; NULL =
- * the default stream).  The first call on a device looks up that array's
- * device address (make it before any stream capture).  Every call shares the
+ * the default stream).  The first call in a CUDA context (normally once per
+ * device) looks up that array's device address: make it before any stream
+ * capture; after cudaDeviceReset the next call looks it up again.  Errors:
+ * BHG_ECUDA only for this call's own lookup or launches (an earlier,
+ * unrelated error on the thread is neither reported nor cleared).  Every call shares the
  * array: calls that overlap on the GPU race and must be serialised (one
  * stream, or events between streams). */
 int bhg_energy_noalloc(const bh_particle64* particles, size_t n, double G, double* result, void* stream);
+
+/* Self-test of the give-up path of the bounded waits.  The radix sort and
+ * the scans wait for their predecessor tiles' look-back words (decoupled
+ * look-back); a wait that sees no word after a bounded number of polls stops,
+ * sets a status bit and lets its kernel finish, so a stalled predecessor
+ * gives BHG_EDEVICE instead of a hung GPU.  This runs that same wait on a
+ * prepared array of 8 tile words, 1..7 published with an aggregate of 1 and
+ * tile 0 published with an inclusive prefix of 1 (publish_first != 0) or never
+ * published, with a poll limit of spin_limit (1 .. 2^20).  Never published:
+ * the wait gives up and the call returns BHG_EDEVICE with the status text;
+ * published: BHG_OK and *prefix (optional) = 8.  The context stays usable
+ * either way.  No counterpart in the reference (its waits are TTG's). */
+int bhg_selftest_wait(bhg_context* ctx, int publish_first, uint32_t spin_limit, uint32_t* prefix);
 
 /* ---- workload generators (synthetic initial conditions) --------------------------- */
 

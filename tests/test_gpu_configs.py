@@ -1,0 +1,159 @@
+"""Parity on the benchmark's own configurations, with the accuracy metric the
+split-precision path is held to: per-particle relative difference from the
+reference's Barnes-Hut forces (rms and 99th percentile, each <= 1e-5), beside
+the global norm of test_bh_vs_bruteforce.cc:30-40.
+
+* The 65,536-particle Plummer sphere (seed 1, eps 0.01, theta 0.5, leaf and
+  target 16, group 256): the build bit for bit, the split and FP64 walks
+  against the oracle's walk, and the 16-step leapfrog schedule (main.cc:199-246)
+  in split precision against the oracle's FP64 schedule.
+* The 4,194,304-particle sphere (seed 2, eps 0.005) and the 2 x 8,388,608
+  merger (seed 4, theta 0.6, eps 0.002): the build bit for bit against the
+  oracle, and the split forces of 4,096 sampled walk targets against the
+  oracle's walk of just those targets (bh_oracle.c bho_walk takes a target list).
+
+The oracle (oracle/bh_oracle.c) is pinned to the reference compiled from its
+own sources (tests/test_oracle_pin.py)."""
+import numpy as np
+import pytest
+
+import bhg
+from helpers import per_particle_rel, rel_error
+from oracle import Params, soa
+
+pytestmark = pytest.mark.gpu
+
+SPLIT_TOL = 1e-5  # per-particle rms, p99 and global, split walk vs the reference's forces
+FP64_TOL = 1e-12  # global, FP64 walk vs the oracle
+# 16 leapfrog steps of dt 1/128 in split precision vs the FP64 oracle: the
+# forces differ by ~1e-7 relative, so positions move apart by ~dt^2 * 1e-7 *
+# |a| per step; 1e-9 in absolute position (the sphere's scale radius is 1)
+SCHEDULE_POS_TOL = 1e-9
+SCHEDULE_VEL_TOL = 1e-8
+
+
+def _oracle_build(oracle, parts, max_leaf):
+    dom, bad = oracle.domain(parts)
+    assert bad == 0
+    keys = oracle.keys(parts, dom)
+    perm, sk = oracle.sort(keys)
+    mp = parts[perm]
+    t = oracle.build(sk, [0], [len(parts)], dom[None], max_leaf, soa(mp))
+    return dom, sk, perm, mp, t
+
+
+def _assert_build_bit_exact(ctx, oracle, parts, max_leaf, group):
+    dom, sk, perm, mp, t = _oracle_build(oracle, parts, max_leaf)
+    ctx.upload(parts)
+    ctx.build_tree(max_leaf, group)
+    ctx.compute_multipoles()
+    assert np.array_equal(ctx.export(bhg.EXPORT_DOMAINS)[0], dom), "domain differs"
+    assert np.array_equal(ctx.export(bhg.EXPORT_KEYS), sk), "sorted keys differ"
+    assert np.array_equal(ctx.export(bhg.EXPORT_PERM), perm), "sort permutation differs"
+    g = ctx.tree()
+    n = t["n"]
+    assert g["n"] == n, f"node count {g['n']} != {n}"
+    for k in ("begin", "count", "first_child", "nchild", "leaf", "depth", "center", "hw", "mass", "com", "iab"):
+        assert np.array_equal(g[k], np.asarray(t[k][:n])), f"node {k} differs"
+    return dom, sk, perm, mp, t
+
+
+def _rel_stats(got, ref):
+    rel = per_particle_rel(got, ref)
+    return {"rms": float(np.sqrt(np.mean(rel ** 2))), "p99": float(np.percentile(rel, 99)),
+            "max": float(rel.max()), "global": rel_error(got, ref)}
+
+
+# ------------------------------------------------------------------ 65,536 Plummer
+
+C0 = dict(n=65536, seed=1, eps=0.01, theta=0.5, leaf=16, target=16, group=256, dt=1.0 / 128, steps=16)
+
+
+@pytest.fixture(scope="module")
+def c0_parts():
+    return bhg.plummer(C0["n"], C0["seed"])[0]
+
+
+def test_c0_build_bit_exact(gpu, oracle, c0_parts):
+    _assert_build_bit_exact(gpu, oracle, c0_parts, C0["leaf"], C0["group"])
+
+
+@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
+def test_c0_walk_matches_oracle(gpu, oracle, c0_parts, precision):
+    eps2 = C0["eps"] ** 2
+    dom, sk, perm, mp, t = _oracle_build(oracle, c0_parts, C0["leaf"])
+    tg = oracle.targets(t, C0["target"], C0["group"])
+    racc, counts = oracle.walk(t, tg, soa(mp), [Params(C0["theta"], eps2, 1.0, 1)] * len(tg))
+    gpu.upload(c0_parts)
+    gpu.stats(reset=True)
+    gpu.build_tree(C0["leaf"], C0["group"])
+    gpu.compute_multipoles()
+    acc = gpu.walk_forces(bhg.Context.params(C0["theta"], eps2, 1.0, True, precision), C0["target"])
+    st = gpu.stats()
+    assert (st["pp"], st["pc"]) == (int(counts[0]), int(counts[1])), "interaction counts differ"
+    s = _rel_stats(acc, racc)
+    print(f"65k precision {precision}: {s}")
+    if precision == bhg.PRECISION_SPLIT:
+        assert s["rms"] <= SPLIT_TOL and s["p99"] <= SPLIT_TOL and s["global"] <= SPLIT_TOL, s
+    else:
+        assert s["global"] <= FP64_TOL, s
+
+
+def _oracle_schedule(oracle, parts, c):
+    eps2 = c["eps"] ** 2
+    dt, steps = c["dt"], c["steps"]
+    ref = parts
+    for k, d in [(dt / 2, dt)] + [(dt, dt)] * (steps - 1) + [(dt / 2, 0.0)]:
+        ref, _, _ = oracle.step(ref, theta=c["theta"], eps2=eps2, max_leaf=c["leaf"], group_size=c["group"],
+                                target_size=c["target"], kick_dt=k, drift_dt=d)
+    return ref
+
+
+@pytest.fixture(scope="module")
+def c0_oracle_schedule(oracle, c0_parts):
+    return _oracle_schedule(oracle, c0_parts, C0)
+
+
+@pytest.mark.parametrize("precision,pos_tol,vel_tol", [(bhg.PRECISION_SPLIT, SCHEDULE_POS_TOL, SCHEDULE_VEL_TOL),
+                                                       (bhg.PRECISION_FP64, 1e-12, 1e-11)])
+def test_c0_schedule_matches_oracle(gpu, c0_parts, c0_oracle_schedule, precision, pos_tol, vel_tol):
+    ref = c0_oracle_schedule
+    gpu.upload(c0_parts)
+    fp = bhg.Context.params(C0["theta"], C0["eps"] ** 2, 1.0, True, precision)
+    gpu.run_schedule(fp, C0["leaf"], C0["group"], C0["target"], C0["dt"], C0["steps"])
+    out = gpu.download()
+    # compared by particle id: a position that differs in its last bits may
+    # fall into the neighbouring Morton cell and change the output order
+    o = out[np.argsort(out["id"])]
+    r = ref[np.argsort(ref["id"])]
+    assert np.array_equal(o["id"], r["id"])
+    dp, dv = np.max(np.abs(o["pos"] - r["pos"])), np.max(np.abs(o["vel"] - r["vel"]))
+    print(f"65k 16-step schedule precision {precision}: max |dpos| {dp:.3e} max |dvel| {dv:.3e}")
+    assert dp <= pos_tol and dv <= vel_tol
+
+
+# ------------------------------------------------------------------ 4M sphere, 16.8M merger
+
+LARGE = {
+    "plummer4m": dict(make=lambda: bhg.plummer(4194304, 2)[0], eps=0.005, theta=0.5),
+    "merger16m": dict(make=lambda: bhg.merger(8388608, 4), eps=0.002, theta=0.6),
+}
+
+
+@pytest.mark.parametrize("name", sorted(LARGE))
+def test_large_build_bit_exact_and_sampled_forces(oracle, name):
+    cfg = LARGE[name]
+    parts = cfg["make"]()
+    eps2 = cfg["eps"] ** 2
+    with bhg.Context(device=0) as ctx:
+        dom, sk, perm, mp, t = _assert_build_bit_exact(ctx, oracle, parts, 16, 256)
+        acc = ctx.walk_forces(bhg.Context.params(cfg["theta"], eps2, 1.0, True, bhg.PRECISION_SPLIT), 16)
+        assert np.array_equal(ctx.export(bhg.EXPORT_TARGETS), oracle.targets(t, 16, 256)), "targets differ"
+    tg = oracle.targets(t, 16, 256)
+    pick = np.sort(np.random.default_rng(2024).choice(len(tg), size=4096, replace=False))
+    sample = tg[pick]
+    racc, _ = oracle.walk(t, sample, soa(mp), [Params(cfg["theta"], eps2, 1.0, 1)] * len(sample))
+    rows = np.concatenate([np.arange(t["begin"][s], t["begin"][s] + t["count"][s]) for s in sample])
+    s = _rel_stats(acc[rows], racc[rows])
+    print(f"{name}: {len(sample)} targets, {len(rows)} particles: {s}")
+    assert s["rms"] <= SPLIT_TOL and s["p99"] <= SPLIT_TOL and s["global"] <= SPLIT_TOL, s

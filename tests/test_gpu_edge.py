@@ -96,3 +96,26 @@ def test_edge_case_matches_oracle(gpu, oracle, name, make, max_leaf, gs, ts, the
             assert rel_error(acc, racc) <= tol
         else:
             assert np.all(acc == 0)
+
+
+def test_bounded_wait_gives_up_and_context_survives(oracle):
+    """The sorts' and scans' look-back wait on a predecessor tile that never
+    publishes (a flag nothing sets) gives up after its poll limit: the kernel
+    finishes, the status bit comes back as BHG_EDEVICE naming the wait, and
+    the context then steps particles normally.  With the predecessor
+    published the same wait returns the full prefix."""
+    with bhg.Context(device=0) as ctx:
+        r, pre = ctx.selftest_wait(True, 1000)
+        assert r == bhg.OK and pre == 8
+        r, _ = ctx.selftest_wait(False, 1000)
+        assert r == bhg.EDEVICE
+        assert "bounded wait" in ctx.last_error()
+        assert ctx.device_status() == 0  # cleared: the next step starts clean
+        parts = cube(2000, 4)
+        out, _, _ = oracle.step(parts, theta=0.5, eps2=1e-6, max_leaf=8, group_size=64, target_size=0)
+        ctx.upload(parts)
+        ctx.step(bhg.Context.params(0.5, 1e-6, 1.0, True, bhg.PRECISION_FP64), 8, 64, 0, 0.0, 0.0)
+        assert np.array_equal(ctx.download()["id"], out["id"])
+        for bad in (0, (1 << 20) + 1):
+            r, _ = ctx.selftest_wait(False, bad)
+            assert r == bhg.EINVAL

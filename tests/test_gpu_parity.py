@@ -349,3 +349,27 @@ def test_energy_conservation_cold_cube(precision):
             ke, pe = ctx.energy()
             drift = max(drift, abs((ke + pe - e0) / e0))
     assert drift <= 0.05, drift
+
+
+@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
+def test_unsoftened_system_among_softened_ones(precision):
+    """Per-system parameters: one system with eps2 0 batched beside softened
+    ones, the step's force params carrying eps2 > 0.  The unsoftened system
+    still gets the reference's r^2 = 0 self-term mask (accumulate_list,
+    grouped_ttg.h:117-123): finite forces, bit for bit those of the system
+    stepped alone with eps2 0."""
+    systems = [bhg.plummer(n, 300 + i)[0] for i, n in enumerate((4000, 2500, 6000))]
+    e2 = np.array([1e-4, 0.0, 1e-4])
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, precision)
+    with bhg.Context(device=0) as mix:
+        mix.upload_systems(systems)
+        mix.set_system_params(theta=np.full(3, 0.5), eps2=e2, kick_dt=np.full(3, 0.01), drift_dt=np.full(3, 0.01))
+        mix.step_systems(fp, 16, 256, 16)
+        out = mix.download()
+    assert np.all(np.isfinite(out["pos"])) and np.all(np.isfinite(out["vel"]))
+    at = sum(len(s) for s in systems[:1])
+    with bhg.Context(device=0) as alone:
+        alone.upload(systems[1])
+        alone.step(bhg.Context.params(0.5, 0.0, 1.0, True, precision), 16, 256, 16, 0.01, 0.01)
+        got = alone.download()
+    assert got.tobytes() == out[at:at + len(systems[1])].tobytes()
