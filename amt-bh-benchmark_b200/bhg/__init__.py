@@ -37,7 +37,7 @@ EXPORTED = (
     "bhg_step_systems_async", "bhg_download_async", "bhg_sync",
     "bhg_run_schedule", "bhg_set_system_params", "bhg_get_stats", "bhg_device_status", "bhg_debug_export",
     "bhg_direct_sum", "bhg_energy", "bhg_energy_noalloc", "bhg_ic_plummer", "bhg_write_csv",
-    "bhg_measure_fp32_peak", "bhg_selftest_wait",
+    "bhg_measure_fp32_peak", "bhg_selftest_wait", "bhg_set_walk_group",
 )
 
 
@@ -128,6 +128,7 @@ def lib() -> C.CDLL:
         "bhg_write_csv": ([C.c_char_p, vp, sz], i32),
         "bhg_measure_fp32_peak": ([i32, C.POINTER(f64)], i32),
         "bhg_selftest_wait": ([vp, i32, u32, C.POINTER(u32)], i32),
+        "bhg_set_walk_group": ([vp, u32], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -419,6 +420,16 @@ class Context:
         out = np.zeros((len(idx), 3))
         self._ck(self.L.bhg_direct_sum(self.h, system, _p(idx), len(idx), eps2, G, _p(out)))
         return out
+
+    #: warps per block of the walk kernels (a compile-time shape)
+    WALK_WARPS = 4
+
+    def set_walk_shape(self, group_particles=0, warps=0):
+        """The walk's shape: the particle cap of a walk group (0 = default 64);
+        warps per block is fixed at WALK_WARPS (0 or that value)."""
+        if warps not in (0, self.WALK_WARPS):
+            raise ValueError(f"the walk kernels run {self.WALK_WARPS} warps per block")
+        self._ck(self.L.bhg_set_walk_group(self.h, group_particles))
 
     def selftest_wait(self, publish_first: bool, spin_limit: int):
         """bhg_selftest_wait: (status code, prefix) of the bounded look-back

@@ -33,11 +33,14 @@ class Pipeline:
     """`counts`: particles per system, back to back in the host buffer the
     steps read and write (pinned, PARTICLE records)."""
 
-    def __init__(self, counts, parts=4, device=0, hbm_budget=0):
+    def __init__(self, counts, parts=4, device=0, hbm_budget=0, walk_group=0):
         self.counts = np.asarray(counts, np.uint64)
         self.runs = split_systems(self.counts, parts)
         offs = np.concatenate([[0], np.cumsum(self.counts.astype(np.int64))])
         self.ctxs = [Context(device=device, hbm_budget=hbm_budget) for _ in self.runs]
+        for c in self.ctxs:
+            if walk_group:
+                c.set_walk_shape(walk_group)
         self.spans = [(int(offs[a]), int(offs[b]), np.ascontiguousarray(self.counts[a:b])) for a, b in self.runs]
 
     def step(self, host_ptr, fp, max_leaf, group_size, target_size, theta, eps2, kick_dt, drift_dt):

@@ -99,15 +99,18 @@ class Server:
     BYTES_PER_PARTICLE each); max_leaf/group_size are the walk's sizes."""
 
     def __init__(self, device=0, hbm_budget=150e9, max_leaf=16, group_size=256, precision=PRECISION_SPLIT,
-                 keep_results=False, on_result=None, max_batch_particles=None):
+                 keep_results=False, on_result=None, max_batch_particles=None, walk_group=0):
         """keep_results: store each finished request's particles in
         self.results[rid]; on_result(rid, particles): hand them to a caller
         instead.  With neither, finished requests leave the GPU uncopied.
         max_batch_particles: a second admission cap, on the particles one
-        tick evaluates (bounds the per-step latency; None = memory only)."""
+        tick evaluates (bounds the per-step latency; None = memory only).
+        walk_group: the walk-group particle cap (0 = the library's default)."""
         # the context's own hard limit leaves room for its fixed tables, the
         # buffers' growth slack and the state's second copy while it grows
         self.ctx = Context(device=device, hbm_budget=int(hbm_budget * 1.15) + (512 << 20))
+        if walk_group:
+            self.ctx.set_walk_shape(walk_group)
         self.budget = hbm_budget
         # the buffers for a full batch up front: admissions then neither
         # allocate nor copy the resident state (without the memory for it

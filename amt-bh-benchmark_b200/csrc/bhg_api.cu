@@ -46,11 +46,11 @@ struct bhg_context {
   // capacities (cap_n covers the scratch, cap_part the state; a capacity is
   // 0 after a growth that failed part-way)
   size_t cap_n = 0, cap_part = 0, cap_nodes = 0, cap_sys = 0, cap_tiles = 0, cap_stiles = 0;
-  // the walk's two-pass schedule: buffers for split_cap groups (0: one pass
-  // only; split_failed: the budget had no room, not tried again)
-  void* split_buf = nullptr;
-  size_t split_cap = 0;
-  bool split_failed = false;
+  // the walk's per-warp lists of sources only some targets of a group take
+  // (list_warps warps' worth), and the particle cap of a walk group
+  void* list_buf = nullptr;
+  size_t list_warps = 0;
+  uint32_t walk_pack = kGroupMax;
 
   // device buffers
   Particle *part = nullptr, *staged = nullptr;
@@ -64,7 +64,7 @@ struct bhg_context {
   SysParam* prm = nullptr;
   Nodes nd{};
   uint32_t *level_lb = nullptr, *mark = nullptr, *targets = nullptr, *scan_lb = nullptr;
-  uint32_t *groups = nullptr, *group_first = nullptr;
+  uint32_t *groups = nullptr, *chunks = nullptr;
   double* accel = nullptr;
   std::vector<std::pair<void*, size_t>> text_scratch;  // cached buffers of the text calls
   DevState* st = nullptr;
@@ -185,14 +185,17 @@ int ensure_nodes(bhg_context* c, size_t need) {
       (r = grow(c, &c->nd.info, cap)) || (r = grow(c, &c->nd.box, cap)) || (r = grow(c, &c->nd.mom, cap)) ||
       (r = grow(c, &c->nd.iab, cap * 6)) || (r = grow(c, &c->nd.w, cap)) || (r = grow(c, &c->nd.q45, cap)) ||
       (r = grow(c, &c->nd.q64, cap * 6)) || (r = grow(c, &c->nd.parent, cap)) || (r = grow(c, &c->nd.upcnt, cap)) ||
-      (r = grow(c, &c->targets, cap)) || (r = grow(c, &c->groups, cap)) ||
-      (r = grow(c, &c->group_first, cap)) ||
+      (r = grow(c, &c->targets, cap)) || (r = grow(c, &c->groups, cap)) || (r = grow(c, &c->chunks, cap)) ||
       (r = grow(c, &c->level_lb, cap / 32 + kLevels + 8)))
     return r;
   c->nd.cap = (uint32_t)cap;
   c->cap_nodes = cap;
   return BHG_OK;
 }
+
+// Look-back words of the three compactions of the walk targets, groups and
+// packing chunks (one word per 4096-item tile each, and some slack).
+size_t scan_words(size_t n) { return 3 * (n / 4096) + 48; }
 
 // Particle-sized buffers and the per-system tables for n particles.  The
 // state (c->part) keeps its first c->n particles across a growth, so
@@ -232,7 +235,7 @@ int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles, size_t n
     // both have the state's capacity
     if ((r = grow(c, &c->staged, c->cap_part)) || (r = grow(c, &c->pm, n)) ||
         (r = grow(c, &c->keys[0], n)) || (r = grow(c, &c->keys[1], n)) || (r = grow(c, &c->vals[0], n)) ||
-        (r = grow(c, &c->vals[1], n)) || (r = grow(c, &c->mark, n)) || (r = grow(c, &c->scan_lb, 2 * (n / 4096) + 32)))
+        (r = grow(c, &c->vals[1], n)) || (r = grow(c, &c->mark, n)) || (r = grow(c, &c->scan_lb, scan_words(n))))
       return r;
     CK(cudaMemsetAsync(c->mark, 0xff, n * sizeof(uint32_t), c->stream));
     c->cap_n = n;
@@ -290,32 +293,37 @@ int walk_grid(bhg_context* c) {
   return c->sms * per;
 }
 
-// Walk groups per resident warp up to which the walk runs its two-pass
-// schedule (k_walk: group walks, then every target walk as a job of its
-// own).  Measured on Plummer spheres: the two passes take 25% less time at
-// 65k particles, 19% at 131k, 10% at 262k, 1% at 524k (37k groups is about
-// 16 per warp) and never more; past that the groups alone keep every warp
-// busy.  The buffers take 3.5 KB per group (136 MB with 2,368 warps).
-constexpr size_t kSplitGroupsPerWarp = 16;
-
-// The buffers of the walk's two-pass schedule, allocated before the walk is
-// captured (walk_grid has also set the kernels' shared-memory limit by
-// then).  Without room for them in the HBM budget the walk keeps the
-// one-pass schedule, which gives the same bits.
+// The walk's per-warp lists (walk_list_cap() 8-byte entries, 64 KB, for
+// every warp of the walk grid: 155 MB on a 148-SM B200), allocated before the
+// walk is captured (walk_grid has also set the kernels' shared-memory limit
+// by then).  Under a tight HBM budget the walk runs on as many blocks as have
+// lists within it (at least one): a group's result does not depend on the
+// warp that walks it, so the bits are the same, only fewer groups at a time.
 int ensure_walk_scratch(bhg_context* c, int grid) {
-  const size_t groups = (size_t)grid * (walk_threads() / 32) * kSplitGroupsPerWarp;
-  if (c->split_cap >= groups || c->split_failed) return BHG_OK;
-  drop_graph(c);
-  dev_free(c, c->split_buf);
-  c->split_buf = nullptr;
-  c->split_cap = 0;
-  if (dev_alloc(c, &c->split_buf, groups * walk_split_bytes_per_group()) != BHG_OK) {
-    c->err.clear();
-    c->split_failed = true;
-    return BHG_OK;
+  const size_t per_warp = walk_list_cap() * sizeof(uint2);
+  const size_t wpb = walk_threads() / 32;
+  size_t warps = (size_t)grid * wpb;
+  if (c->list_warps >= warps) return BHG_OK;
+  if (c->budget) {
+    const size_t held = c->list_warps * per_warp;  // freed below, so it counts as room
+    const size_t room = c->budget > c->allocated - held ? c->budget - (c->allocated - held) : 0;
+    warps = std::min(warps, std::max(wpb, room / per_warp / wpb * wpb));
+    if (c->list_warps >= warps) return BHG_OK;
   }
-  c->split_cap = groups;
+  drop_graph(c);
+  dev_free(c, c->list_buf);
+  c->list_buf = nullptr;
+  c->list_warps = 0;
+  int r = dev_alloc(c, &c->list_buf, warps * per_warp);
+  if (r) return r;
+  c->list_warps = warps;
   return BHG_OK;
+}
+
+// Blocks of the walk launch: the occupancy grid, or fewer when the lists
+// were limited by the HBM budget.
+int walk_launch_grid(bhg_context* c) {
+  return (int)std::min<size_t>((size_t)walk_grid(c), c->list_warps / (walk_threads() / 32));
 }
 
 // Lays out the systems c->counts back to back with their sort tiles, sizes
@@ -438,12 +446,9 @@ void enq_moments(bhg_context* c) {
 void enq_targets(bhg_context* c, uint32_t target_size) {
   cudaStream_t s = c->stream;
   cudaMemsetAsync(reinterpret_cast<char*>(c->st) + kWalkResetOffset, 0, sizeof(DevState) - kWalkResetOffset, s);
-  cudaMemsetAsync(c->scan_lb, 0, (2 * (c->n / 4096) + 32) * sizeof(uint32_t), s);
+  cudaMemsetAsync(c->scan_lb, 0, scan_words(c->n) * sizeof(uint32_t), s);
   const uint32_t lim = std::min(target_size, c->group_size);
-  // walk groups share the upper walk of their targets; with targets above
-  // kGroupMax particles every target is its own group
-  const uint32_t glim = std::max<uint32_t>(lim, kGroupMax);
-  launch_targets(c->nd, lim, glim, (uint32_t)c->n, c->mark, c->targets, c->groups, c->group_first, c->scan_lb, c->st,
+  launch_targets(c->nd, lim, c->walk_pack, (uint32_t)c->n, c->mark, c->targets, c->chunks, c->groups, c->scan_lb, c->st,
                  c->sms, s);
 }
 
@@ -458,7 +463,6 @@ void enq_walk(bhg_context* c, bool want_accel) {
   a.pm = c->pm;
   a.targets = c->targets;
   a.groups = c->groups;
-  a.group_first = c->group_first;
   a.sys = c->sys;
   a.prm = c->prm;
   a.nsys = c->nsys;
@@ -466,11 +470,8 @@ void enq_walk(bhg_context* c, bool want_accel) {
   a.out = c->part;
   a.accel = want_accel ? c->accel : nullptr;
   a.st = c->st;
-  a.gsum = static_cast<double*>(c->split_buf);
-  a.gdefer = reinterpret_cast<uint32_t*>(a.gsum + c->split_cap * kGroupMax * 3);
-  a.gnd = a.gdefer + c->split_cap * walk_defer_cap();
-  a.split_max = (uint32_t)c->split_cap;
-  launch_walk(a, c->precision, c->quad != 0, c->mask, walk_grid(c), c->stream);
+  a.wlist = static_cast<uint2*>(c->list_buf);
+  launch_walk(a, c->precision, c->quad != 0, c->mask, walk_launch_grid(c), c->stream);
   launch_eval_done(c->st, c->stream);
 }
 
@@ -558,8 +559,8 @@ int run_phase(bhg_context* c, int phase, bool graphed, const std::string& key, F
 
 std::string graph_key(const bhg_context* c, uint32_t target_size) {
   char key[192];
-  snprintf(key, sizeof key, "%zu/%d/%zu/%zu/%u/%u/%u/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->split_cap,
-           c->max_leaf, c->group_size, target_size, c->precision, c->quad, (int)c->mask);
+  snprintf(key, sizeof key, "%zu/%d/%zu/%zu/%u/%u/%u/%u/%d/%d/%d", c->n, c->nsys, c->cap_nodes, c->list_warps,
+           c->walk_pack, c->max_leaf, c->group_size, target_size, c->precision, c->quad, (int)c->mask);
   return key;
 }
 
@@ -1382,10 +1383,10 @@ int bhg_get_stats(bhg_context* c, bhg_stats* out, int reset) {
   out->sort_passes = kSortPasses;
   // bounds + domain + keys + digit offsets; the sort passes; gather + roots +
   // one per level; the multipoles (one kernel, or one per level); mark +
-  // compact of the targets and of the groups + first target per group; walk
-  // (+ its target pass) + its completion count
-  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (c->n <= kMomentsOneLaunchMax ? 1 : kMortonDepth + 1) + 5 +
-                          2 + (c->split_cap ? 1 : 0);
+  // compact of the targets, packing + compact of the walk groups; walk + its
+  // completion count
+  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (c->n <= kMomentsOneLaunchMax ? 1 : kMortonDepth + 1) + 4 +
+                          2;
   if (reset) {
     for (double& t : c->tot_ms) t = 0.0;
     c->walks_timed = 0;
@@ -1535,6 +1536,16 @@ int bhg_energy(bhg_context* c, int sys, double G, double* kinetic, double* poten
   for (uint32_t b = 0; b < blocks; ++b) ek += h[2 * b], ep += h[2 * b + 1];
   if (kinetic) *kinetic = ek;
   if (potential) *potential = ep;
+  return BHG_OK;
+}
+
+int bhg_set_walk_group(bhg_context* c, uint32_t particles) {
+  if (!c) return BHG_EINVAL;
+  if (particles > (uint32_t)kGroupMax)
+    return fail(c, BHG_EINVAL, "a walk group holds at most " + std::to_string(kGroupMax) + " particles");
+  const uint32_t p = particles ? particles : (uint32_t)kGroupMax;
+  if (p != c->walk_pack) drop_graph(c);
+  c->walk_pack = p;
   return BHG_OK;
 }
 

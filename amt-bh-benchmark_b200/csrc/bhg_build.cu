@@ -501,9 +501,8 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(int depth, Nodes nd, co
 // ---------------------------------------------------------------------------
 // Cuts of the tree: the topmost nodes that are leaves or hold at most `lim`
 // particles, marked at their first particle and compacted in Morton order.
-// Used twice per walk: for the walk targets (lim = min(target_size,
-// group_size)) and for the walk groups (lim = kGroupMax), the nodes whose
-// targets share the upper part of their walk.
+// Used for the walk targets (lim = min(target_size, group_size)); the same
+// compaction then lists the walk groups (k_pack_groups).
 
 __global__ void k_mark_cut(Nodes nd, uint32_t lim, const DevState* __restrict__ st, uint32_t* __restrict__ mark) {
   if (st->status & kStNodeOverflow) return;  // children may lie beyond the slots
@@ -570,21 +569,69 @@ __global__ void __launch_bounds__(kScanThreads) k_compact(uint32_t* __restrict__
   }
 }
 
-// first_target[g]: index of the first target inside group g (targets and
-// groups are both in Morton order and every target lies inside one group).
-__global__ void k_group_first(const uint32_t* __restrict__ groups, const uint32_t* __restrict__ targets,
-                              const uint32_t* __restrict__ nbegin, const DevState* __restrict__ st,
-                              uint32_t* __restrict__ first_target) {
-  const uint32_t ng = st->n_groups, nt = st->n_targets;
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
-    const uint32_t gb = nbegin[groups[g]];
+// Walk groups: runs of consecutive targets (Morton order) that share one
+// traversal.  Any set of targets may share one: a node accepted for the
+// bounding box of all their particles is accepted for each target's box
+// inside it, and a node rejected for every point of that box is opened by
+// each target (mac_accept_bbox / mac_reject_all, multipole.h:158-160), so
+// every target still gets exactly its own interaction list.  A group holds at
+// most `pack` (<= kGroupMax) particles and kMaxTargets targets, and a target
+// larger than `pack` is a group of its own.  The targets are packed greedily
+// inside packing chunks - the topmost tree nodes of at most kPackChunk
+// particles (or leaves) - one warp per chunk: a chunk lies inside one system
+// and its targets depend on that system alone, so a system's groups, and
+// with them its results bit for bit, do not depend on the other systems of
+// the context.  Group starts are marked at their first target's index for
+// the compaction.
+constexpr uint32_t kPackChunk = 2048;
+
+__global__ void k_pack_groups(const uint32_t* __restrict__ chunks, const uint32_t* __restrict__ targets,
+                              const uint32_t* __restrict__ nbegin, const uint32_t* __restrict__ ncount,
+                              uint32_t pack, const DevState* __restrict__ st, uint32_t* __restrict__ mark) {
+  if (st->status & kStNodeOverflow) return;
+  const uint32_t nchunks = st->n_chunks, nt = st->n_targets;
+  const int lane = threadIdx.x & 31;
+  const uint32_t wpb = blockDim.x >> 5;
+  for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < nchunks; c += gridDim.x * wpb) {
+    const uint32_t cn = chunks[c];
+    const uint32_t cb = nbegin[cn], ce = cb + ncount[cn];
+    // the chunk's first target: the first whose particles start at or after cb
     uint32_t lo = 0, hi = nt;
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
-      if (nbegin[targets[mid]] < gb) lo = mid + 1;
+      if (nbegin[targets[mid]] < cb) lo = mid + 1;
       else hi = mid;
     }
-    first_target[g] = lo;
+    uint32_t cnt = 0, k = 0;
+    bool first = true;
+    for (uint32_t t0 = lo;; t0 += 32) {
+      const uint32_t t = t0 + lane;
+      uint32_t n = 0xffffffffu;  // past the chunk
+      if (t < nt) {
+        const uint32_t tn = targets[t];
+        if (nbegin[tn] < ce) n = ncount[tn];
+      }
+      // the greedy packing, run alike by every lane over the 32 counts
+      uint32_t starts = 0;
+      bool end = false;
+      for (int i = 0; i < 32; ++i) {
+        const uint32_t ni = __shfl_sync(0xffffffffu, n, i);
+        if (ni == 0xffffffffu) {
+          end = true;
+          break;
+        }
+        if (first || cnt + ni > pack || k >= (uint32_t)kMaxTargets) {
+          starts |= 1u << i;
+          cnt = 0;
+          k = 0;
+          first = false;
+        }
+        cnt += ni;
+        ++k;
+      }
+      if ((starts >> lane) & 1u) mark[t] = t;
+      if (end) break;
+    }
   }
 }
 
@@ -785,16 +832,17 @@ void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_
 // Grids of the cut kernels (tiles and nodes taken by grid stride or by a
 // counter): measured at 4M, the targets phase takes 0.179 ms with 4/2/2
 // blocks per SM and 0.140 with 16/8/8.
-void launch_targets(const Nodes& nd, uint32_t lim, uint32_t group_lim, uint32_t n, uint32_t* mark, uint32_t* targets,
-                    uint32_t* groups, uint32_t* first_target, uint32_t* lookback, DevState* st, int sms,
-                    cudaStream_t s) {
+void launch_targets(const Nodes& nd, uint32_t lim, uint32_t pack, uint32_t n, uint32_t* mark, uint32_t* targets,
+                    uint32_t* chunks, uint32_t* groups, uint32_t* lookback, DevState* st, int sms, cudaStream_t s) {
   const uint32_t ntiles = (n + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
   k_mark_cut<<<sms * 16, 256, 0, s>>>(nd, lim, st, mark);
   k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, targets, lookback, &st->scan_tiles, &st->n_targets, st);
-  k_mark_cut<<<sms * 16, 256, 0, s>>>(nd, group_lim, st, mark);
-  k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, groups, lookback + ntiles + 8, &st->group_tiles,
+  k_mark_cut<<<sms * 16, 256, 0, s>>>(nd, kPackChunk, st, mark);
+  k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, chunks, lookback + (ntiles + 8), &st->chunk_tiles,
+                                             &st->n_chunks, st);
+  k_pack_groups<<<sms * 4, 256, 0, s>>>(chunks, targets, nd.begin, nd.count, pack, st, mark);
+  k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, groups, lookback + 2 * (ntiles + 8), &st->group_tiles,
                                              &st->n_groups, st);
-  k_group_first<<<sms * 8, 256, 0, s>>>(groups, targets, nd.begin, st, first_target);
 }
 
 // Per-level multipoles at 16 blocks of 128 per SM: 0.233 ms at 4M, 0.270

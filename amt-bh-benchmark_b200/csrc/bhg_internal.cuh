@@ -99,7 +99,8 @@ struct DevState {
   uint32_t walk_next;        // next group of the walk
   uint32_t scan_tiles;       // tiles taken by the target compaction
   uint32_t group_tiles;      // tiles taken by the group compaction
-  uint32_t walk_next2;       // next target of the walk's second pass
+  uint32_t n_chunks;         // packing chunks of the walk groups
+  uint32_t chunk_tiles;      // tiles taken by the chunk compaction
   unsigned long long pp, pc;  // interaction counts of the walk
 };
 constexpr size_t kBuildResetOffset = offsetof(DevState, n_nodes);
@@ -145,6 +146,7 @@ constexpr uint32_t kNoParent = 0xffffffffu;
 // Kernel-launch helpers shared by the .cu files (defined in bhg_build.cu).
 constexpr int kTile = 4096;  // particles per radix-sort / bounds tile
 constexpr int kSortPasses = 8;
-constexpr int kGroupMax = 64;  // particles of a walk group (targets sharing one upper walk)
+constexpr int kGroupMax = 64;    // particles of a walk group (targets sharing one traversal)
+constexpr int kMaxTargets = 32;  // targets of a walk group (the bits of a traversal mask)
 
 }  // namespace bhg

@@ -29,12 +29,14 @@ void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_
 // holds at most target_size particles (grouped_ttg.h:253); on every
 // root-to-leaf path that is the deeper of the two cuts, i.e. the first node
 // with count <= min(target_size, group_size).  group_size 0 (the per-node
-// pass) and target_size 0 both give the leaves.  The walk groups are the
-// same cut at group_lim (>= lim): the nodes whose targets share the upper
-// part of one walk; first_target[g] is the index of group g's first target.
-void launch_targets(const Nodes& nd, uint32_t lim, uint32_t group_lim, uint32_t n, uint32_t* mark, uint32_t* targets,
-                    uint32_t* groups, uint32_t* first_target, uint32_t* lookback, DevState* st, int sms,
-                    cudaStream_t s);
+// pass) and target_size 0 both give the leaves.  The walk groups are runs of
+// consecutive targets of one system, at most `pack` particles and
+// kMaxTargets targets each (a larger target alone), packed inside chunks of
+// the tree (chunks: node-sized scratch): groups[g] is the index of group g's
+// first target, st->n_groups their number.  lookback: 3 regions of
+// n / 4096 + 9 words.
+void launch_targets(const Nodes& nd, uint32_t lim, uint32_t pack, uint32_t n, uint32_t* mark, uint32_t* targets,
+                    uint32_t* chunks, uint32_t* groups, uint32_t* lookback, DevState* st, int sms, cudaStream_t s);
 // one_launch: k_moments_up (one kernel, children-first by counters) instead of
 // one kernel per level; the same bits either way
 void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, bool one_launch, cudaStream_t s);
@@ -48,8 +50,7 @@ struct WalkArgs {
   const uint32_t* ncount;
   const double4* pm;
   const uint32_t* targets;
-  const uint32_t* groups;
-  const uint32_t* group_first;  // first target of each group
+  const uint32_t* groups;  // first target of each walk group
   const SysDev* sys;
   const SysParam* prm;
   int nsys;
@@ -57,12 +58,9 @@ struct WalkArgs {
   Particle* out;           // kicked/drifted particles (the state)
   double* accel;           // optional: G*a, 3 per particle
   DevState* st;
-  // the two-pass schedule for few walk groups (k_walk): groups' shared
-  // parts (kGroupMax x 3 per group), deferred nodes, deferred counts
-  double* gsum;
-  uint32_t* gdefer;
-  uint32_t* gnd;
-  uint32_t split_max;  // two passes when n_groups <= split_max (0: never)
+  // per-warp lists of the sources only some targets of a group take
+  // (walk_list_cap() entries per warp of the grid)
+  uint2* wlist;
 };
 
 // Walks every target and kicks/drifts its particles.  precision:
@@ -70,9 +68,8 @@ struct WalkArgs {
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s);
 int walk_blocks_per_sm(int precision, bool quad, bool mask);
 int walk_threads();
-// device bytes per group of the two-pass schedule's buffers; deferred slots per group
-size_t walk_split_bytes_per_group();
-size_t walk_defer_cap();
+// entries of one warp's partial-source list
+size_t walk_list_cap();
 
 void launch_integrate(Particle* p, const double* accel, uint32_t n, const SysDev* sys, const SysParam* prm, int nsys,
                       int sms, cudaStream_t s);

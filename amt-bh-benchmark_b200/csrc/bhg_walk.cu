@@ -43,22 +43,28 @@ constexpr int kWalkWarps = 4;
 constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kCellQ = 128;   // ring of accepted cells (a batch of up to 64 + one step's 32)
 constexpr int kPartQ = 256;   // ring of direct particles (a batch of up to 192 + 32 enqueued)
-constexpr int kStackCap = 1024;  // per-warp shared-memory stack
-constexpr int kDeferCap = 512;   // per-warp deferred nodes of a group walk
+constexpr int kStackCap = 704;   // per-warp stack: node + target mask per entry
 constexpr int kStageF4 = 3 * 64 + 3;  // staged source records (float4): 64 cells + the zero cell
 constexpr float kFarAway = 1.0e10f;  // padding source: contributes exactly 0
 constexpr uint32_t kFull = 0xffffffffu;
-static_assert(kStackCap >= kDeferCap + 7 * kLevels + 1 + 32, "a DFS walk from the deferred nodes must fit");
+constexpr uint32_t kLeafBit = 0x80000000u;  // list entry: a leaf whose particles some targets take
+constexpr uint32_t kListCap = 8192;         // entries of one warp's partial-source list
+// a walk that pops one node at a time holds at most 7 entries per level
+// below the one it pops from, plus the root
+static_assert(kStackCap >= 7 * kLevels + 1 + 8, "a one-at-a-time walk must fit the stack");
 static_assert(kStageF4 * 16 >= 32 * 6 * 8, "the end-of-walk reduction reuses the staging records");
 
 struct WarpSmem {
-  uint32_t stack[kStackCap];
-  uint32_t defer[kDeferCap];
+  uint32_t snode[kStackCap];  // traversal stack: node
+  uint32_t smask[kStackCap];  //                  targets that still need it
   uint32_t cell[kCellQ];
   uint32_t part[kPartQ];
   float4 stage[kStageF4];
   double acc[kGroupMax][3];   // FP64 sum per particle of the group
-  double tacc[kGroupMax][3];  // FP64 sums of one target's own walk
+  double tlo[kMaxTargets][3], thi[kMaxTargets][3];  // the targets' particle boxes
+  double glo[3], ghi[3];                              // the group's particle box
+  uint32_t tbeg[kMaxTargets], tcnt[kMaxTargets];      // the targets' particles
+  uint32_t accbits[32];  // per popped entry: targets that accept it (per-target tests)
 };
 constexpr size_t kWalkSmem = sizeof(WarpSmem) * kWalkWarps;
 
@@ -489,85 +495,107 @@ struct F64Eval {
 };
 
 // ---------------------------------------------------------------------------
-// One traversal.  GROUP mode (the shared group walk): accepted -> cells,
-// rejected for the whole box -> opened, otherwise deferred to S.defer.
-// TARGET mode: accepted -> cells, otherwise opened.  The walk starts from
-// the root (nstart == 0) or from the nstart deferred nodes.  Returns 1 if
-// the stack would overflow (redo popping one node at a time, which bounds
-// it), 2 if the deferred list would overflow (GROUP mode: give up sharing).
+// Source queues shared by every traversal below.  Accepted cells go to a ring
+// of node ids and opened leaves' particles to a ring of particle indices; a
+// full ring (or the end of the walk) is evaluated as one batch.  A loop
+// iteration does exactly one thing: evaluate a cell batch, evaluate a
+// particle batch, enqueue up to 32 particles of the leaves opened last, or
+// let the producer (a traversal step, a list scan) add sources.  The
+// evaluators are reached from this one place each (their bodies would
+// otherwise be inlined many times over).
 
-enum { kModeTarget = 0, kModeGroup = 1 };
-
-// The evaluators are reached from exactly one call site each (their bodies
-// are specialised on the live target count and would otherwise be inlined
-// many times over): the step loop below alternates between appending to
-// the queues and evaluating one queue chunk, and k_walk runs every walk of a
-// group through one call of walk_and_sum.
-template <class E>
-__device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, uint32_t nstart,
-                                 const double lo[3], const double hi[3], double theta2, bool group_mode, bool dfs,
-                                 int lane, unsigned long long& ncells, unsigned long long& nparts, uint32_t& ndefer) {
-  const int C = ev.cell_chunk(), CP = ev.part_chunk();  // sources per evaluated batch
-  const uint32_t lt = lanemask_lt();
-  uint32_t top;
-  if (nstart == 0) {
-    if (lane == 0) S.stack[0] = root;
-    top = 1;
-  } else {
-    for (uint32_t i = lane; i < nstart; i += 32) S.stack[i] = S.defer[i];
-    top = nstart;
-  }
-  __syncwarp();
+struct Queues {
   uint32_t chead = 0, phead = 0;
   int ncell = 0, npart = 0;
-  ncells = nparts = 0;
-  ndefer = 0;
-  // a walk pops each node at most once: more steps than nodes means a
-  // corrupt tree
+  // particles of the leaves opened by the last producer step, still to enqueue
+  uint32_t ptot = 0, pbase = 0, pinc = 0, pc = 0, pfirst = 0;
+  unsigned long long ncells = 0, nparts = 0;  // sources evaluated
+};
+
+// Appends the lanes' accepted cells (one per lane where `take`).
+__device__ __forceinline__ void push_cells(WarpSmem& S, Queues& q, bool take, uint32_t node, uint32_t lt) {
+  const uint32_t am = __ballot_sync(kFull, take);
+  if (take) S.cell[(q.chead + q.ncell + __popc(am & lt)) & (kCellQ - 1)] = node;
+  q.ncell += __popc(am);
+}
+
+// Records the lanes' opened leaves (cnt particles from `first`; cnt 0 = none):
+// their particles are enqueued by the next loop iterations.
+__device__ __forceinline__ void open_leaves(Queues& q, uint32_t cnt, uint32_t first, int lane) {
+  q.pc = cnt;
+  q.pinc = warp_incl_scan_u32(cnt, lane);
+  q.ptot = __shfl_sync(kFull, q.pinc, 31);
+  q.pbase = 0;
+  q.pfirst = first;
+}
+
+// One iteration's queue work; returns false when the producer should run
+// (queues below a batch and no particles left to enqueue), true otherwise.
+// `more`: the producer has more to add.
+template <class E>
+__device__ __forceinline__ bool drain_step(E& ev, WarpSmem& S, Queues& q, bool more, int lane) {
+  const bool done = !more && q.pbase >= q.ptot;
+  const int C = ev.cell_chunk(), CP = ev.part_chunk();
+  if (q.ncell >= C || (done && q.ncell > 0)) {
+    const int c = min(q.ncell, C);
+    ev.cells(S.cell, q.chead, c);
+    q.chead += c;
+    q.ncell -= c;
+    q.ncells += c;
+    return true;
+  }
+  if (q.npart >= CP || (done && q.npart > 0)) {
+    const int c = min(q.npart, CP);
+    ev.parts(S.part, q.phead, c);
+    q.phead += c;
+    q.npart -= c;
+    q.nparts += c;
+    return true;
+  }
+  if (q.pbase < q.ptot) {  // enqueue up to 32 particles of the opened leaves
+    const uint32_t idx = q.pbase + lane;
+    uint32_t src = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const uint32_t v = __shfl_sync(kFull, q.pinc, (src + step - 1) & 31);
+      if (v <= idx) src += step;
+    }
+    src = min(src, 31u);
+    const uint32_t sf = __shfl_sync(kFull, q.pfirst, src);
+    const uint32_t sinc = __shfl_sync(kFull, q.pinc, src);
+    const uint32_t spc = __shfl_sync(kFull, q.pc, src);
+    const uint32_t take = min(32u, q.ptot - q.pbase);
+    if ((uint32_t)lane < take) S.part[(q.phead + q.npart + lane) & (kPartQ - 1)] = sf + (idx - (sinc - spc));
+    q.npart += take;
+    q.pbase += take;
+    __syncwarp();
+    return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Walk of one target's particle box from the root (the reference's
+// per-target list): accepted -> cells, otherwise opened (leaves contribute
+// their particles, interior nodes push their children).  Used for targets of
+// more than kGroupMax particles (in batches of kGroupMax targets) and for the
+// targets of a group whose shared walk outgrew its list.  Returns 1 if the
+// stack would overflow (redo popping one node at a time, which bounds it).
+
+template <class E>
+__device__ __forceinline__ int target_walk(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, const double lo[3],
+                                           const double hi[3], double theta2, bool dfs, int lane, Queues& q) {
+  const uint32_t lt = lanemask_lt();
+  if (lane == 0) S.snode[0] = root;
+  uint32_t top = 1;
+  __syncwarp();
+  q = Queues();
+  // a walk pops each node at most once: more steps than nodes means a corrupt tree
   uint32_t steps = 0;
   const uint32_t max_steps = a.st->n_nodes + 2;
-  // particles of the leaves opened by the current step, still to enqueue
-  uint32_t ptot = 0, pbase = 0, pinc = 0, pc = 0, pfirst = 0;
   for (;;) {
-    const bool done = top == 0 && pbase >= ptot;
-    // 1. one chunk of work: a cell chunk, a particle chunk, or enqueue
-    if (ncell >= C || (done && ncell > 0)) {
-      const int c = min(ncell, C);
-      ev.cells(S.cell, chead, c);
-      chead += c;
-      ncell -= c;
-      ncells += c;
-      continue;
-    }
-    if (npart >= CP || (done && npart > 0)) {
-      const int c = min(npart, CP);
-      ev.parts(S.part, phead, c);
-      phead += c;
-      npart -= c;
-      nparts += c;
-      continue;
-    }
-    if (done) break;
-    if (pbase < ptot) {  // enqueue up to 32 particles of the opened leaves
-      const uint32_t idx = pbase + lane;
-      uint32_t src = 0;
-#pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const uint32_t v = __shfl_sync(kFull, pinc, (src + step - 1) & 31);
-        if (v <= idx) src += step;
-      }
-      src = min(src, 31u);
-      const uint32_t sf = __shfl_sync(kFull, pfirst, src);
-      const uint32_t sinc = __shfl_sync(kFull, pinc, src);
-      const uint32_t spc = __shfl_sync(kFull, pc, src);
-      const uint32_t take = min(32u, ptot - pbase);
-      if ((uint32_t)lane < take) S.part[(phead + npart + lane) & (kPartQ - 1)] = sf + (idx - (sinc - spc));
-      npart += take;
-      pbase += take;
-      __syncwarp();
-      continue;
-    }
-    // 2. one traversal step: pop up to 32 nodes and classify them
+    if (drain_step(ev, S, q, top > 0, lane)) continue;
+    if (top == 0) break;
     if (++steps > max_steps) {
       if (lane == 0) atomicOr(&a.st->status, kStWalkLimit);
       top = 0;
@@ -576,53 +604,185 @@ __device__ __forceinline__ int walk(E& ev, const WalkArgs& a, WarpSmem& S, uint3
     const uint32_t n = dfs ? 1u : min(top, 32u);
     top -= n;
     const bool valid = (uint32_t)lane < n;
-    const uint32_t node = valid ? S.stack[top + lane] : 0u;
+    const uint32_t node = valid ? S.snode[top + lane] : 0u;
     __syncwarp();
-    bool accept = false, open = false, leaf = false;
+    bool accept = false, leaf = false;
     uint32_t first = 0, cnt = 0, info = 0;
     if (valid) {
       const WNode* w = a.w + node;
       const double4 c4 = *reinterpret_cast<const double4*>(&w->cx);  // com xyz, edge^2
       const uint4 u4 = *reinterpret_cast<const uint4*>(&w->first);   // first, count, info, mass
-      first = u4.x;
-      cnt = u4.y;
-      info = u4.z;
+      first = u4.x, cnt = u4.y, info = u4.z;
       leaf = info_leaf(info);
       // mac_accept_bbox: theta^2 * near^2 > edge^2 (multipole.h:151-153)
       accept = __dmul_rn(theta2, near2(lo, hi, c4.x, c4.y, c4.z)) > c4.w;
-      if (!accept) {
-        // group walk: mac_reject_all, theta^2 * far^2 <= edge^2 (multipole.h:158-160)
-        open = !group_mode || __dmul_rn(theta2, far2(lo, hi, c4.x, c4.y, c4.z)) <= c4.w;
-      }
     }
-    // accepted: cell queue
-    const uint32_t am = __ballot_sync(kFull, accept);
-    if (accept) S.cell[(chead + ncell + __popc(am & lt)) & (kCellQ - 1)] = node;
-    ncell += __popc(am);
-    if (group_mode) {  // neither: deferred to the targets
-      const bool defer = valid && !accept && !open;
-      const uint32_t dm = __ballot_sync(kFull, defer);
-      if (ndefer + __popc(dm) > (uint32_t)kDeferCap) return 2;
-      if (defer) S.defer[ndefer + __popc(dm & lt)] = node;
-      ndefer += __popc(dm);
-    }
-    // opened interior nodes: push the children
-    const uint32_t nch = (open && !leaf) ? info_nchild(info) : 0u;
+    push_cells(S, q, accept, node, lt);
+    const uint32_t nch = (valid && !accept && !leaf) ? info_nchild(info) : 0u;
     const uint32_t cinc = warp_incl_scan_u32(nch, lane);
     const uint32_t ctot = __shfl_sync(kFull, cinc, 31);
     if (top + ctot > (uint32_t)kStackCap) return 1;
-    for (uint32_t k = 0; k < nch; ++k) S.stack[top + cinc - nch + k] = first + k;
+    for (uint32_t k = 0; k < nch; ++k) S.snode[top + cinc - nch + k] = first + k;
     top += ctot;
-    // opened leaves: their particles, enqueued by the next iterations
-    pc = (open && leaf) ? cnt : 0u;
-    pinc = warp_incl_scan_u32(pc, lane);
-    ptot = __shfl_sync(kFull, pinc, 31);
-    pbase = 0;
-    pfirst = first;
+    open_leaves(q, (valid && !accept && leaf) ? cnt : 0u, first, lane);
     __syncwarp();
   }
   __syncwarp();
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The shared walk of a group of k <= kMaxTargets targets (particles p0 ..
+// p0 + np - 1, np <= kGroupMax), in the spirit of GroupWalker::visit
+// (grouped_ttg.h:204-289) taken to every level: one traversal from the root
+// whose stack entries carry the mask of targets that still need the node.
+// Each popped node is first tested against the group's particle box:
+// accepted there (mac_accept_bbox) -> accepted by every target in the mask;
+// rejected for every point of it (mac_reject_all, multipole.h:158-160) ->
+// opened by every target in the mask; otherwise each target in the mask
+// tests its own box, one (node, target) pair per lane.  A node taken by every
+// target of the group goes to the group queues and is evaluated once against
+// all np particles; one taken by some targets only goes to the warp's list as
+// (node, mask) for the targets' own passes (target_pass).  Opened interior
+// nodes push their children with the mask of the targets that opened them.
+// Every target's list is exactly what a walk of its own box from the root
+// gives (multipole.h's tests are monotone in the box).
+// Returns 0, 1 (stack overflow: redo popping one node at a time) or 2 (list
+// overflow: the targets walk on their own).
+
+template <class E>
+__device__ __forceinline__ int group_walk(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, uint32_t k,
+                                          double theta2, bool dfs, int lane, uint2* list, uint32_t& nlist, Queues& q) {
+  const uint32_t lt = lanemask_lt();
+  const uint32_t full = k == 32 ? kFull : ((1u << k) - 1u);
+  if (lane == 0) S.snode[0] = root, S.smask[0] = full;
+  uint32_t top = 1;
+  __syncwarp();
+  q = Queues();
+  nlist = 0;
+  uint32_t steps = 0;
+  const uint32_t max_steps = a.st->n_nodes + 2;
+  for (;;) {
+    if (drain_step(ev, S, q, top > 0, lane)) continue;
+    if (top == 0) break;
+    if (++steps > max_steps) {
+      if (lane == 0) atomicOr(&a.st->status, kStWalkLimit);
+      top = 0;
+      continue;
+    }
+    // pop up to 32 entries, fewer when the stack is nearly full (each popped
+    // node pushes at most 8)
+    uint32_t n = dfs ? 1u : min(top, 32u);
+    if (!dfs) n = min(n, max((kStackCap - top) / 7u, 1u));
+    top -= n;
+    const bool valid = (uint32_t)lane < n;
+    uint32_t node = 0, mask = 0;
+    if (valid) node = S.snode[top + lane], mask = S.smask[top + lane];
+    __syncwarp();
+    double4 c4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    uint4 u4 = make_uint4(0u, 0u, 0u, 0u);
+    bool acc = false, rej = false;
+    if (valid) {
+      const WNode* w = a.w + node;
+      c4 = *reinterpret_cast<const double4*>(&w->cx);
+      u4 = *reinterpret_cast<const uint4*>(&w->first);
+      acc = __dmul_rn(theta2, near2(S.glo, S.ghi, c4.x, c4.y, c4.z)) > c4.w;
+      // one target: its box is the group's, so not accepted means opened
+      if (!acc) rej = k == 1 || __dmul_rn(theta2, far2(S.glo, S.ghi, c4.x, c4.y, c4.z)) <= c4.w;
+    }
+    uint32_t A = acc ? mask : 0u, O = rej ? mask : 0u;
+    // undecided nodes: every target in the mask tests its own box
+    const bool und = valid && !acc && !rej;
+    const uint32_t pcnt = und ? (uint32_t)__popc(mask) : 0u;
+    const uint32_t pincl = warp_incl_scan_u32(pcnt, lane);
+    const uint32_t ptotal = __shfl_sync(kFull, pincl, 31);
+    if (ptotal) {
+      S.accbits[lane] = 0u;
+      __syncwarp();
+      for (uint32_t base = 0; base < ptotal; base += 32) {
+        const uint32_t j = base + (uint32_t)lane;
+        // the entry holding pair j: the first lane whose inclusive count exceeds j
+        uint32_t e = 0;
+#pragma unroll
+        for (int st = 16; st >= 1; st >>= 1) {
+          const uint32_t v = __shfl_sync(kFull, pincl, (e + st - 1) & 31);
+          if (v <= j) e += st;
+        }
+        e = min(e, 31u);
+        const uint32_t einc = __shfl_sync(kFull, pincl, e), ecnt = __shfl_sync(kFull, pcnt, e);
+        uint32_t em = __shfl_sync(kFull, mask, e);
+        const double ex = __shfl_sync(kFull, c4.x, e), ey = __shfl_sync(kFull, c4.y, e);
+        const double ez = __shfl_sync(kFull, c4.z, e), ee = __shfl_sync(kFull, c4.w, e);
+        if (j < ptotal) {
+          // target t: the r-th set bit of the entry's mask
+          uint32_t r = j - (einc - ecnt), t = 0;
+#pragma unroll
+          for (int wdt = 16; wdt >= 1; wdt >>= 1) {
+            const uint32_t low = (uint32_t)__popc(em & ((1u << wdt) - 1u));
+            if (r >= low) r -= low, em >>= wdt, t += wdt;
+          }
+          if (__dmul_rn(theta2, near2(S.tlo[t], S.thi[t], ex, ey, ez)) > ee) atomicOr(&S.accbits[e], 1u << t);
+        }
+      }
+      __syncwarp();
+      if (und) A = S.accbits[lane], O = mask & ~A;
+      __syncwarp();
+    }
+    const bool leaf = valid && info_leaf(u4.z);
+    // sources every target takes: the group queues
+    push_cells(S, q, A != 0u && A == full, node, lt);
+    // sources some targets take: the list
+    const bool cpart = A != 0u && A != full, lpart = leaf && O != 0u && O != full;
+    const uint32_t nl = (cpart ? 1u : 0u) + (lpart ? 1u : 0u);
+    const uint32_t linc = warp_incl_scan_u32(nl, lane);
+    const uint32_t ltot = __shfl_sync(kFull, linc, 31);
+    if (nlist + ltot > kListCap) return 2;
+    uint32_t at = nlist + linc - nl;
+    if (cpart) list[at++] = make_uint2(node, A);
+    if (lpart) list[at] = make_uint2(node | kLeafBit, O);
+    nlist += ltot;
+    // opened interior nodes: children, with the targets that opened them
+    const uint32_t nch = (O != 0u && !leaf) ? info_nchild(u4.z) : 0u;
+    const uint32_t cinc = warp_incl_scan_u32(nch, lane);
+    const uint32_t ctot = __shfl_sync(kFull, cinc, 31);
+    if (top + ctot > (uint32_t)kStackCap) return 1;
+    for (uint32_t c = 0; c < nch; ++c) S.snode[top + cinc - nch + c] = u4.x + c, S.smask[top + cinc - nch + c] = O;
+    top += ctot;
+    // leaves every target opens: their particles, for the group queues
+    open_leaves(q, (leaf && O == full) ? u4.y : 0u, u4.x, lane);
+    __syncwarp();
+  }
+  __syncwarp();
+  return 0;
+}
+
+// Target `bit` of the group takes, from the list, the entries whose mask
+// holds it: cells into its cell queue, leaves' particles into its particle
+// queue; evaluated with the evaluator set up for its particles.
+template <class E>
+__device__ __forceinline__ void target_pass(E& ev, const WalkArgs& a, WarpSmem& S, const uint2* list, uint32_t nlist,
+                                            uint32_t bit, int lane, Queues& q) {
+  const uint32_t lt = lanemask_lt();
+  q = Queues();
+  uint32_t at = 0;
+  for (;;) {
+    if (drain_step(ev, S, q, at < nlist, lane)) continue;
+    if (at >= nlist) break;
+    const uint32_t j = at + (uint32_t)lane;
+    const uint2 e = j < nlist ? list[j] : make_uint2(0u, 0u);
+    const bool hit = (e.y >> bit) & 1u;
+    const bool isleaf = (e.x & kLeafBit) != 0u;
+    push_cells(S, q, hit && !isleaf, e.x, lt);
+    uint32_t first = 0, cnt = 0;
+    if (hit && isleaf) {
+      const uint2 fc = *reinterpret_cast<const uint2*>(&a.w[e.x & ~kLeafBit].first);
+      first = fc.x, cnt = fc.y;
+    }
+    open_leaves(q, cnt, first, lane);
+    at += 32;
+    __syncwarp();
+  }
+  __syncwarp();
 }
 
 // Bounding box of particles [b, b + T) (BBox::add, multipole.h:121-128).
@@ -646,31 +806,16 @@ __device__ __forceinline__ void particle_box(const double4* pm, uint32_t b, uint
   }
 }
 
-// Evaluates the walk of the targets [p0, p0 + tb) (tb <= 64) into the FP64
-// sums[0 .. tb), zeroed first (and again if the walk is redone).
-template <class E>
-__device__ __forceinline__ int walk_and_sum(E& ev, const WalkArgs& a, WarpSmem& S, double (*sums)[3], uint32_t root,
-                                            uint32_t nstart, const double lo[3], const double hi[3], double theta2,
-                                            bool group_mode, uint32_t p0, int tb, int lane, unsigned long long& n_pp,
-                                            unsigned long long& n_pc, bool quad, uint32_t& ndefer) {
-  unsigned long long nc = 0, np = 0;
-  int r = 0;
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    for (int t = lane; t < tb; t += 32) sums[t][0] = sums[t][1] = sums[t][2] = 0.0;
-    __syncwarp();
-    ev.setup(lane, p0, tb, sums);
-    r = walk(ev, a, S, root, nstart, lo, hi, theta2, group_mode, attempt == 1, lane, nc, np, ndefer);
-    if (r != 1) break;
-  }
-  if (r == 2) return 2;  // GROUP mode only: the caller discards this walk
-  ev.finish();
+// The interaction counts of one evaluated list: quad -> cells are
+// particle-cell interactions, else monopoles counted as particle-particle.
+__device__ __forceinline__ void add_counts(const Queues& q, uint32_t targets, bool quad, unsigned long long& n_pp,
+                                      unsigned long long& n_pc) {
   if (quad) {
-    n_pc += nc * (unsigned long long)tb;
-    n_pp += np * (unsigned long long)tb;
+    n_pc += q.ncells * (unsigned long long)targets;
+    n_pp += q.nparts * (unsigned long long)targets;
   } else {
-    n_pp += (nc + np) * (unsigned long long)tb;
+    n_pp += (q.ncells + q.nparts) * (unsigned long long)targets;
   }
-  return 0;
 }
 
 // on_result(particle, G * acc) (grouped_ttg.h:281-283), then kick_one /
@@ -711,166 +856,142 @@ __device__ __forceinline__ uint32_t system_of(const WalkArgs& a, uint32_t p) {
   return lo;
 }
 
-constexpr uint32_t kNotShared = 0xffffffffu;  // the group walk gave up: targets walk from the root
+// Every target of the group [t0, t1) (particles p0 .. p0 + np) walks on its
+// own from the root into S.acc (the group walk outgrew its list).
+template <class E, bool QUAD>
+__device__ void targets_alone(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, double theta2, uint32_t k,
+                              uint32_t p0, int lane, unsigned long long& n_pp, unsigned long long& n_pc) {
+  Queues q;
+  for (uint32_t i = 0; i < k; ++i) {
+    const uint32_t tb = S.tbeg[i], tn = S.tcnt[i];
+    ev.cx = 0.5 * (S.tlo[i][0] + S.thi[i][0]), ev.cy = 0.5 * (S.tlo[i][1] + S.thi[i][1]);
+    ev.cz = 0.5 * (S.tlo[i][2] + S.thi[i][2]);
+    int r = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      ev.setup(lane, tb, (int)tn, S.acc + (tb - p0));
+      r = target_walk(ev, a, S, root, S.tlo[i], S.thi[i], theta2, attempt == 1, lane, q);
+      if (r == 0) break;
+    }
+    ev.finish();
+    add_counts(q, tn, QUAD, n_pp, n_pc);
+  }
+}
 
-// One warp per walk group.  The walks of a group - its shared group walk,
-// then one per target (one per kGroupMax particles of a large leaf target) -
-// run as consecutive jobs through a single walk_and_sum call.
-//
-// With few groups (n_groups <= a.split_max: about as many groups as warps,
-// so the largest group would set the kernel's time) the work is cut in two
-// passes instead: this kernel runs the group walks (and the groups that are
-// their own target) and leaves each group's shared part and deferred nodes
-// in a.gsum / a.gdefer / a.gnd; k_walk_targets then runs every target walk
-// as a job of its own.  Both schedules run the same walks and add the
-// target's part onto the group's part the same way, so the results are the
-// same bits.
+// One warp per walk group (a run of targets, k_pack_groups).  A group of one
+// target larger than kGroupMax particles walks in batches of kGroupMax
+// targets.  Otherwise: the group's shared walk with every source all its
+// targets take evaluated against all its particles, then each target's pass
+// over the list of the sources only some take, each adding its part onto the
+// group's FP64 sums in target order; then the kick/drift.
 template <class E, bool QUAD>
 __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
   if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;  // the build failed: touch nothing
+  uint2* list = a.wlist + (size_t)(blockIdx.x * kWalkWarps + warp) * kListCap;
   const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
-  const bool two_pass = ngroups <= a.split_max;
   unsigned long long n_pp = 0, n_pc = 0;
   E ev(a, S.stage, lane);
+  Queues q;
   for (;;) {
     uint32_t gi = 0;
     if (lane == 0) gi = atomicAdd(&a.st->walk_next, 1u);
     gi = __shfl_sync(kFull, gi, 0);
     if (gi >= ngroups) break;
-    const uint32_t gnode = a.groups[gi];
-    const uint32_t gb = a.nbegin[gnode], gn = a.ncount[gnode];
-    const uint32_t s = a.nsys > 1 ? system_of(a, gb) : 0u;
+    const uint32_t t0 = a.groups[gi], t1 = gi + 1 < ngroups ? a.groups[gi + 1] : ntargets;
+    const uint32_t k = t1 - t0;
+    const uint32_t first_node = a.targets[t0];
+    const uint32_t p0 = a.nbegin[first_node];
+    const uint32_t s = a.nsys > 1 ? system_of(a, p0) : 0u;
     const uint32_t root = a.sys[s].root;
     const SysParam& sp = a.prm[s];
     const double theta2 = sp.theta2;
     ev.set_system(sp.eps2, a.sys[s].hw);
-    uint32_t ti = a.group_first[gi];
-    const bool single = ti < ntargets && a.targets[ti] == gnode;  // the group is its own target
-    bool group_job = !single, shared = false;
-    uint32_t ndefer = 0, tb = gb, T = gn, b0 = 0;
-    double lo[3], hi[3];
-    particle_box(a.pm, gb, gn, lane, lo, hi);
-    for (;;) {
-      // -- the next job: the group walk, or (a batch of) the next target
-      if (!group_job) {
-        if (b0 == 0) {
-          if (!single) {
-            if (ti >= ntargets) break;
-            const uint32_t tnode = a.targets[ti];
-            tb = a.nbegin[tnode];
-            T = a.ncount[tnode];
-            if (tb >= gb + gn || (shared && ndefer == 0)) break;  // past the group, or nothing deferred
-            particle_box(a.pm, tb, T, lane, lo, hi);
-          }
-        }
-      }
-      const uint32_t p0 = group_job ? gb : tb + b0;
-      const int nt = (int)(group_job ? gn : min((uint32_t)kGroupMax, T - b0));
-      double(*sums)[3] = (group_job || single) ? S.acc : S.tacc;
+    const uint32_t n0 = a.ncount[first_node];
+    if (k == 1 && n0 > (uint32_t)kGroupMax) {
+      // a large target: batches of kGroupMax particles, each walking the
+      // whole target's box from the root
+      double lo[3], hi[3];
+      particle_box(a.pm, p0, n0, lane, lo, hi);
       ev.cx = 0.5 * (lo[0] + hi[0]), ev.cy = 0.5 * (lo[1] + hi[1]), ev.cz = 0.5 * (lo[2] + hi[2]);
-      uint32_t nd = 0;
-      const int r = walk_and_sum(ev, a, S, sums, root, (!group_job && shared) ? ndefer : 0u, lo, hi, theta2, group_job,
-                                 p0, nt, lane, n_pp, n_pc, QUAD, nd);
-      // -- what the job leaves behind
-      if (group_job) {
-        group_job = false;
-        shared = r == 0;
-        ndefer = nd;
-        if (!shared) {  // too many deferred nodes: every target walks from the root
-          for (uint32_t i = lane; i < gn; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
-          __syncwarp();
+      for (uint32_t b0 = 0; b0 < n0; b0 += kGroupMax) {
+        const uint32_t nb = min((uint32_t)kGroupMax, n0 - b0);
+        for (uint32_t i = lane; i < nb; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
+        __syncwarp();
+        int r = 0;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+          ev.setup(lane, p0 + b0, (int)nb, S.acc);
+          r = target_walk(ev, a, S, root, lo, hi, theta2, attempt == 1, lane, q);
+          if (r == 0) break;
         }
-        if (two_pass) {  // the targets walk in k_walk_targets
-          double* g = a.gsum + (size_t)gi * (kGroupMax * 3);
-          for (uint32_t i = lane; i < gn; i += 32) g[3 * i] = S.acc[i][0], g[3 * i + 1] = S.acc[i][1], g[3 * i + 2] = S.acc[i][2];
-          if (shared)
-            for (uint32_t i = lane; i < ndefer; i += 32) a.gdefer[(size_t)gi * kDeferCap + i] = S.defer[i];
-          if (lane == 0) a.gnd[gi] = shared ? ndefer : kNotShared;
-          __syncwarp();
-          break;
-        }
-        continue;
+        ev.finish();
+        add_counts(q, nb, QUAD, n_pp, n_pc);
+        kick_drift(a, sp, S.acc, p0 + b0, nb, lane);
       }
-      if (single) {  // a batch of a large target is written out right away
-        kick_drift(a, sp, S.acc, p0, (uint32_t)nt, lane);
-        b0 += kGroupMax;
-        if (b0 >= T) break;
-        continue;
-      }
-      for (int i = lane; i < nt; i += 32) {  // the target's own part onto the group's shared part
-        double* d = S.acc[p0 - gb + (uint32_t)i];
-        d[0] += S.tacc[i][0], d[1] += S.tacc[i][1], d[2] += S.tacc[i][2];
-      }
-      __syncwarp();
-      ++ti;
+      continue;
     }
-    if (!single && !two_pass) kick_drift(a, sp, S.acc, gb, gn, lane);
-  }
-  if (lane == 0) {
-    atomicAdd(&a.st->pp, n_pp);
-    atomicAdd(&a.st->pc, n_pc);
-  }
-}
-
-// The second pass of the two-pass schedule (see k_walk): one warp per target
-// of a group that is not its own target, walking from the group's deferred
-// nodes; the target's part goes onto the group's shared part, then kick/drift.
-template <class E, bool QUAD>
-__global__ void __launch_bounds__(kWalkThreads, 4) k_walk_targets(WalkArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;
-  const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
-  if (ngroups > a.split_max) return;  // k_walk ran the one-pass schedule
-  unsigned long long n_pp = 0, n_pc = 0;
-  E ev(a, S.stage, lane);
-  for (;;) {
-    uint32_t ti = 0;
-    if (lane == 0) ti = atomicAdd(&a.st->walk_next2, 1u);
-    ti = __shfl_sync(kFull, ti, 0);
-    if (ti >= ntargets) break;
-    // its group: the last one whose first target is at or before ti
-    uint32_t gi = 0, hi = ngroups;
-    while (hi - gi > 1) {
-      const uint32_t mid = (gi + hi) >> 1;
-      if (a.group_first[mid] <= ti) gi = mid;
-      else hi = mid;
-    }
-    const uint32_t gnode = a.groups[gi];
-    if (a.targets[a.group_first[gi]] == gnode) continue;  // its own target: done in the first pass
-    const uint32_t tnode = a.targets[ti];
-    const uint32_t tb = a.nbegin[tnode], T = a.ncount[tnode];  // T <= kGroupMax: inside a group
-    const uint32_t gb = a.nbegin[gnode];
-    const uint32_t s = a.nsys > 1 ? system_of(a, tb) : 0u;
-    const SysParam& sp = a.prm[s];
-    const uint32_t nd = a.gnd[gi];
-    const bool shared = nd != kNotShared;
-    const double* g = a.gsum + (size_t)gi * (kGroupMax * 3) + 3 * (size_t)(tb - gb);
-    if (shared && nd == 0) {  // nothing deferred: the group's part is the whole sum
-      for (uint32_t i = lane; i < T; i += 32) S.tacc[i][0] = g[3 * i], S.tacc[i][1] = g[3 * i + 1], S.tacc[i][2] = g[3 * i + 2];
-    } else {
-      if (shared)
-        for (uint32_t i = lane; i < nd; i += 32) S.defer[i] = a.gdefer[(size_t)gi * kDeferCap + i];
-      __syncwarp();
-      ev.set_system(sp.eps2, a.sys[s].hw);
-      double lo[3], hi3[3];
-      particle_box(a.pm, tb, T, lane, lo, hi3);
-      ev.cx = 0.5 * (lo[0] + hi3[0]), ev.cy = 0.5 * (lo[1] + hi3[1]), ev.cz = 0.5 * (lo[2] + hi3[2]);
-      uint32_t nd2 = 0;
-      walk_and_sum(ev, a, S, S.tacc, a.sys[s].root, shared ? nd : 0u, lo, hi3, sp.theta2, false, tb, (int)T, lane, n_pp,
-                   n_pc, QUAD, nd2);
-      for (uint32_t i = lane; i < T; i += 32) {  // the target's own part onto the group's shared part
-        S.tacc[i][0] = g[3 * i] + S.tacc[i][0];
-        S.tacc[i][1] = g[3 * i + 1] + S.tacc[i][1];
-        S.tacc[i][2] = g[3 * i + 2] + S.tacc[i][2];
+    // the targets: particle ranges and boxes (lane i: target i), the group box
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if ((uint32_t)lane < k) {
+      const uint32_t tn = a.targets[t0 + lane];
+      const uint32_t tb = a.nbegin[tn], tc = a.ncount[tn];
+      for (uint32_t i = 0; i < tc; ++i) {
+        const double4 p = a.pm[tb + i];
+        lo[0] = fmin(lo[0], p.x), hi[0] = fmax(hi[0], p.x);
+        lo[1] = fmin(lo[1], p.y), hi[1] = fmax(hi[1], p.y);
+        lo[2] = fmin(lo[2], p.z), hi[2] = fmax(hi[2], p.z);
       }
+      S.tbeg[lane] = tb, S.tcnt[lane] = tc;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) S.tlo[lane][d] = lo[d], S.thi[lane][d] = hi[d];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], o));
+        hi[d] = fmax(hi[d], __shfl_xor_sync(kFull, hi[d], o));
+      }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) S.glo[d] = lo[d], S.ghi[d] = hi[d];
     }
     __syncwarp();
-    kick_drift(a, sp, S.tacc, tb, T, lane);
+    const uint32_t np = S.tbeg[k - 1] + S.tcnt[k - 1] - p0;
+    for (uint32_t i = lane; i < np; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
+    __syncwarp();
+    // the shared walk (redone one node at a time if the stack would overflow)
+    ev.cx = 0.5 * (lo[0] + hi[0]), ev.cy = 0.5 * (lo[1] + hi[1]), ev.cz = 0.5 * (lo[2] + hi[2]);
+    uint32_t nlist = 0;
+    int r = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      ev.setup(lane, p0, (int)np, S.acc);
+      r = group_walk(ev, a, S, root, k, theta2, attempt == 1, lane, list, nlist, q);
+      if (r != 1) break;
+    }
+    if (r == 0) {
+      ev.finish();
+      add_counts(q, np, QUAD, n_pp, n_pc);
+      // each target's part from the list, in target order
+      if (nlist) {
+        for (uint32_t i = 0; i < k; ++i) {
+          const uint32_t tb = S.tbeg[i], tn = S.tcnt[i];
+          ev.cx = 0.5 * (S.tlo[i][0] + S.thi[i][0]), ev.cy = 0.5 * (S.tlo[i][1] + S.thi[i][1]);
+          ev.cz = 0.5 * (S.tlo[i][2] + S.thi[i][2]);
+          ev.setup(lane, tb, (int)tn, S.acc + (tb - p0));
+          target_pass(ev, a, S, list, nlist, i, lane, q);
+          ev.finish();
+          add_counts(q, tn, QUAD, n_pp, n_pc);
+        }
+      }
+    } else {
+      // the list overflowed: nothing of the shared walk is kept (its partial
+      // sums were never added); every target walks on its own
+      targets_alone<E, QUAD>(ev, a, S, root, theta2, k, p0, lane, n_pp, n_pc);
+    }
+    kick_drift(a, sp, S.acc, p0, np, lane);
   }
   if (lane == 0) {
     atomicAdd(&a.st->pp, n_pp);
@@ -881,7 +1002,6 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk_targets(WalkArgs a) {
 template <class E, bool QUAD>
 static void launch_one(const WalkArgs& a, int grid, cudaStream_t s) {
   k_walk<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
-  if (a.split_max) k_walk_targets<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
 }
 
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s) {
@@ -897,7 +1017,6 @@ void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int gri
 template <class E, bool QUAD>
 static int occ() {
   cudaFuncSetAttribute(k_walk<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
-  cudaFuncSetAttribute(k_walk_targets<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
   int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<E, QUAD>, kWalkThreads, kWalkSmem);
   return b > 0 ? b : 1;
@@ -923,8 +1042,7 @@ int walk_blocks_per_sm(int precision, bool quad, bool mask) {
 
 int walk_threads() { return kWalkThreads; }
 
-size_t walk_split_bytes_per_group() { return kGroupMax * 3 * sizeof(double) + kDeferCap * sizeof(uint32_t) + sizeof(uint32_t); }
-size_t walk_defer_cap() { return kDeferCap; }
+size_t walk_list_cap() { return kListCap; }
 
 // ---------------------------------------------------------------------------
 // Unfused integrate phase: kick_one / drift_one (integrate.h:15-16) with

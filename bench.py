@@ -78,6 +78,13 @@ SORT_BYTES_PER_PASS = 24  # read + write of an 8-byte key and a 4-byte index
 FLOPS_PP, FLOPS_PC = 20, 60
 
 
+def TUNE_CANDIDATES():
+    """The autotuner's search space: leaf (= target) size x walk-group cap."""
+    from bhg import autotune
+
+    return autotune.candidates(leaves=(16, 24, 32, 48), walk_groups=(32, 64))
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -568,11 +575,13 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
     ns = len(systems)
     n = sum(len(p) for p in systems)
     eps2 = w["eps"] ** 2
-    tuned = autotune.tune(systems, w["theta"], eps2, w["group"], bhg.PRECISION_SPLIT, device=rig.local)
+    tuned = autotune.tune(systems, w["theta"], eps2, w["group"], bhg.PRECISION_SPLIT, device=rig.local,
+                          cands=TUNE_CANDIDATES())
     leaf = tuned["max_leaf"]
     fp = bhg.Context.params(w["theta"], eps2, 1.0, True, bhg.PRECISION_SPLIT)
     ctx = bhg.Context(device=rig.local)
     ctx.set_stream(rig.stream.cuda_stream)
+    ctx.set_walk_shape(tuned["walk_group"])
     ctx.upload_systems(systems)
     ones = np.ones(ns)
 
@@ -587,7 +596,8 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
     ps = rig.sum_over_ranks(n * args.steps)
     out = {"value": ps / (ms / 1000.0), "ms_per_step": ms / args.steps, "clocks": clocks,
            **roofline(st, n, fp32_peak, peaks),
-           "autotune": {k: tuned[k] for k in ("max_leaf", "target_size", "rms_error", "err_budget", "table")}}
+           "autotune": {k: tuned[k] for k in ("max_leaf", "target_size", "walk_group", "rms_error", "err_budget",
+                                               "table")}}
 
     if not args.no_e2e:
         flat = np.concatenate(systems)
@@ -609,7 +619,7 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
         from bhg.pipeline import Pipeline
 
         host[:] = flat
-        pipe = Pipeline(counts, parts=args.pipe_parts, device=rig.local)
+        pipe = Pipeline(counts, parts=args.pipe_parts, device=rig.local, walk_group=tuned["walk_group"])
 
         def pipe_step():
             pipe.step(ptr, fp, leaf, w["group"], leaf, w["theta"], eps2, w["dt"], w["dt"])
@@ -807,7 +817,7 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks, quick=False):
         allp = c.download()
     offs = np.cumsum([0] + [r.n for r in sample])
     tuned = autotune.tune([allp[offs[i]:offs[i + 1]] for i in range(len(sample))], 0.5, w["eps"] ** 2, w["group"],
-                          bhg.PRECISION_SPLIT, device=rig.local)
+                          bhg.PRECISION_SPLIT, device=rig.local, cands=TUNE_CANDIDATES())
     leaf = tuned["max_leaf"]
     # warm-up: a few small requests through the same loop (kernels loaded,
     # occupancy queried)
@@ -821,7 +831,7 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks, quick=False):
         delivered[0] += 1
 
     srv = serve.Server(device=rig.local, hbm_budget=w["hbm_budget_gb"] * 1e9, max_leaf=leaf,
-                       group_size=w["group"], on_result=on_result,
+                       group_size=w["group"], on_result=on_result, walk_group=tuned["walk_group"],
                        max_batch_particles=w.get("max_batch_particles"))
     srv.ctx.stats(reset=True)
     rig.barrier()
@@ -871,7 +881,8 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks, quick=False):
                 out["force_error"] = force_error(c, parts, fp, leaf, w["group"], leaf, pick.eps ** 2)
             out["force_error"]["system"] = f"request {pick.rid}: {pick.kind}, N={pick.n}, theta 0.5, leaf {leaf}"
     out["config_extra"] = {"mean_particles_per_tick": n_eval, "max_leaf_tuned": leaf}
-    out["autotune"] = {k: tuned[k] for k in ("max_leaf", "target_size", "rms_error", "err_budget", "table")}
+    out["autotune"] = {k: tuned[k] for k in ("max_leaf", "target_size", "walk_group", "rms_error", "err_budget",
+                                             "table")}
     out["autotune"]["sample"] = f"{len(sample)} of the stream's first 64 requests, {tot} particles, theta 0.5"
     return out
 

@@ -246,6 +246,14 @@ int bhg_run_schedule(bhg_context* ctx, const bhg_force_params* fp, unsigned max_
 int bhg_set_system_params(bhg_context* ctx, const double* theta, const double* eps2, const double* kick_dt,
                           const double* drift_dt);
 
+/* The particle cap of one walk group (1 .. 64; 0 = the default, 64).  The
+ * walk runs one warp per group of consecutive walk targets of one system;
+ * the group's targets share one traversal of the tree (each still gets
+ * exactly the reference's own list, GroupWalker, grouped_ttg.h:204-289), so
+ * larger groups share more, smaller ones give more groups to spread over
+ * the GPU.  Results are reproducible bit for bit for a given cap. */
+int bhg_set_walk_group(bhg_context* ctx, uint32_t particles);
+
 /* Blocks.  reset != 0 starts new sums after reading. */
 int bhg_get_stats(bhg_context* ctx, bhg_stats* out, int reset);
 /* Device-side status bits of the last step (0 = fine); blocks. */

@@ -148,20 +148,20 @@ def test_quadrupole_beats_monopole(gpu, oracle, precision):
 
 
 @pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-12), (bhg.PRECISION_SPLIT, 1e-5)])
-def test_deferral_overflow_falls_back(oracle, precision, tol):
-    """theta 0.2 on a uniform cube with one particle per leaf: some group walks
-    defer more nodes than a group's deferred list holds (up to ~1,200 against
-    512), so those groups' targets walk from the root, and walks outgrow the
-    stack and are redone one node at a time.  Lists and forces still match
-    the oracle's, in the two-pass and the one-pass schedule alike."""
-    parts = cube(8000, 5)
-    theta, eps2 = 0.2, 1e-6
+def test_list_overflow_falls_back(oracle, precision, tol):
+    """theta 0.15 on a uniform cube with one particle per leaf: for about one
+    group in five the sources only some of its targets take outgrow the
+    warp's list (8,192 entries), and those groups' targets walk on their own
+    from the root.  Lists and forces still match the oracle's, for every
+    walk-group size."""
+    parts = cube(20000, 5)
+    theta, eps2 = 0.15, 1e-6
     dom, sk, perm, mp, t = _oracle_build(oracle, parts, 1)
     tg = oracle.targets(t, 1, 64)
     racc, counts = oracle.walk(t, tg, soa(mp), [Params(theta, eps2, 1.0, 1)] * len(tg))
-    accs = []
-    for budget in (0, 32 << 20):  # unlimited: two passes; 32 MB: no room for that buffer, one pass
-        with bhg.Context(device=0, hbm_budget=budget) as ctx:
+    for group in (64, 8):
+        with bhg.Context(device=0) as ctx:
+            ctx.set_walk_shape(group)
             ctx.upload(parts)
             ctx.build_tree(1, 64)
             ctx.compute_multipoles()
@@ -169,9 +169,45 @@ def test_deferral_overflow_falls_back(oracle, precision, tol):
             st = ctx.stats()
             assert (st["pp"], st["pc"]) == (int(counts[0]), int(counts[1])), "interaction counts differ"
             assert rel_error(acc, racc) <= tol
-            accs.append((acc, st["kernels_per_eval"]))
-    assert accs[0][1] == accs[1][1] + 1  # the two schedules ran
-    assert accs[0][0].tobytes() == accs[1][0].tobytes()
+
+
+@pytest.mark.parametrize("precision,tol", [(bhg.PRECISION_FP64, 1e-12), (bhg.PRECISION_SPLIT, 1e-5)])
+@pytest.mark.parametrize("group", [1, 5, 16, 33, 64])
+def test_walk_group_sizes_match_oracle(gpu, oracle, precision, tol, group):
+    """Any walk-group cap gives every target exactly its own list (the
+    interaction counts equal the oracle's) and the oracle's forces."""
+    parts = bhg.plummer(30000, 31)[0]
+    dom, sk, perm, mp, t = _oracle_build(oracle, parts, 16)
+    tg = oracle.targets(t, 16, 256)
+    racc, counts = oracle.walk(t, tg, soa(mp), [Params(0.5, 1e-4, 1.0, 1)] * len(tg))
+    gpu.set_walk_shape(group)
+    try:
+        gpu.upload(parts)
+        gpu.stats(reset=True)
+        gpu.build_tree(16, 256)
+        gpu.compute_multipoles()
+        acc = gpu.walk_forces(bhg.Context.params(0.5, 1e-4, 1.0, True, precision), 16)
+        st = gpu.stats()
+    finally:
+        gpu.set_walk_shape(0)
+    assert (st["pp"], st["pc"]) == (int(counts[0]), int(counts[1])), "interaction counts differ"
+    assert rel_error(acc, racc) <= tol
+
+
+@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
+def test_budget_limited_walk_grid_same_bits(precision):
+    """Under a tight HBM budget the walk runs on fewer blocks (as many as
+    have their lists within the budget): the same bits as on the full grid."""
+    parts = bhg.plummer(30000, 31)[0]
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, precision)
+    out = {}
+    for budget in (0, 40 << 20):
+        with bhg.Context(device=0, hbm_budget=budget) as ctx:
+            ctx.upload(parts)
+            for _ in range(2):
+                ctx.step(fp, 16, 256, 16, 0.01, 0.01)
+            out[budget] = ctx.download()
+    assert out[0].tobytes() == out[40 << 20].tobytes()
 
 
 def test_no_softening_masks_self(gpu, oracle):
@@ -305,26 +341,6 @@ def test_system_alone_equals_in_the_mix(precision):
             got = alone.download()
             assert got.tobytes() == out[at:at + len(s)].tobytes()
             at += len(s)
-
-
-@pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
-def test_two_pass_walk_equals_one_pass(precision):
-    """With few walk groups the walk runs group walks first and every target
-    walk as a job of its own (two kernels); without room for that schedule's
-    buffers (a tight HBM budget) it runs one warp per group.  Same bits."""
-    parts = bhg.plummer(30000, 31)[0]
-    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, precision)
-    out, stats = {}, {}
-    for budget in (0, 14 << 20):
-        with bhg.Context(device=0, hbm_budget=budget) as ctx:
-            ctx.upload(parts)
-            for _ in range(2):
-                ctx.step(fp, 16, 256, 16, 0.01, 0.01)
-            out[budget] = ctx.download()
-            stats[budget] = ctx.stats()
-    assert stats[0]["kernels_per_eval"] == stats[14 << 20]["kernels_per_eval"] + 1  # the two schedules ran
-    assert (stats[0]["pp"], stats[0]["pc"]) == (stats[14 << 20]["pp"], stats[14 << 20]["pc"])
-    assert out[0].tobytes() == out[14 << 20].tobytes()
 
 
 @pytest.mark.parametrize("precision", [bhg.PRECISION_FP64, bhg.PRECISION_SPLIT])
