@@ -293,35 +293,40 @@ int walk_grid(bhg_context* c) {
   return c->sms * per;
 }
 
-// The walk's per-warp lists (walk_list_cap() 8-byte entries, 64 KB, for
-// every warp of the walk grid: 155 MB on a 148-SM B200), allocated before the
-// walk is captured (walk_grid has also set the kernels' shared-memory limit
-// by then).  Under a tight HBM budget the walk runs on as many blocks as have
-// lists within it (at least one): a group's result does not depend on the
-// warp that walks it, so the bits are the same, only fewer groups at a time.
+// The walk's list slots (walk_slot_bytes(), ~34 KB each): two per warp of
+// the walk grid (161 MB on a 148-SM B200) - one list per warp in the one-pass
+// schedule, one per group in the two-pass schedule, which therefore serves
+// up to two groups per warp.  Allocated before the walk is captured
+// (walk_grid has also set the kernels' shared-memory limit by then).  Under
+// a tight HBM budget there are fewer slots and the walk runs on as many
+// blocks as have a slot per warp (at least one block): a group's result does
+// not depend on the warp that walks it nor on the schedule, so the bits are
+// the same, only fewer groups at a time.
+constexpr size_t kSlotsPerWarp = 2;
+
 int ensure_walk_scratch(bhg_context* c, int grid) {
-  const size_t per_warp = walk_list_cap() * sizeof(uint2);
+  const size_t per_slot = walk_slot_bytes();
   const size_t wpb = walk_threads() / 32;
-  size_t warps = (size_t)grid * wpb;
-  if (c->list_warps >= warps) return BHG_OK;
+  size_t slots = (size_t)grid * wpb * kSlotsPerWarp;
+  if (c->list_warps >= slots) return BHG_OK;
   if (c->budget) {
-    const size_t held = c->list_warps * per_warp;  // freed below, so it counts as room
+    const size_t held = c->list_warps * per_slot;  // freed below, so it counts as room
     const size_t room = c->budget > c->allocated - held ? c->budget - (c->allocated - held) : 0;
-    warps = std::min(warps, std::max(wpb, room / per_warp / wpb * wpb));
-    if (c->list_warps >= warps) return BHG_OK;
+    slots = std::min(slots, std::max(wpb, room / per_slot / wpb * wpb));
+    if (c->list_warps >= slots) return BHG_OK;
   }
   drop_graph(c);
   dev_free(c, c->list_buf);
   c->list_buf = nullptr;
   c->list_warps = 0;
-  int r = dev_alloc(c, &c->list_buf, warps * per_warp);
+  int r = dev_alloc(c, &c->list_buf, slots * per_slot);
   if (r) return r;
-  c->list_warps = warps;
+  c->list_warps = slots;
   return BHG_OK;
 }
 
-// Blocks of the walk launch: the occupancy grid, or fewer when the lists
-// were limited by the HBM budget.
+// Blocks of the walk launch: the occupancy grid, or fewer when the HBM
+// budget limited the slots (one per warp at least).
 int walk_launch_grid(bhg_context* c) {
   return (int)std::min<size_t>((size_t)walk_grid(c), c->list_warps / (walk_threads() / 32));
 }
@@ -470,7 +475,12 @@ void enq_walk(bhg_context* c, bool want_accel) {
   a.out = c->part;
   a.accel = want_accel ? c->accel : nullptr;
   a.st = c->st;
+  // slots: the lists, then the groups' sums, then the list lengths
+  a.nslots = (uint32_t)c->list_warps;
   a.wlist = static_cast<uint2*>(c->list_buf);
+  a.gsum = reinterpret_cast<double*>(reinterpret_cast<char*>(c->list_buf) +
+                                     c->list_warps * (walk_slot_bytes() - kGroupMax * 3 * sizeof(double) - sizeof(uint32_t)));
+  a.gnl = reinterpret_cast<uint32_t*>(a.gsum + c->list_warps * kGroupMax * 3);
   launch_walk(a, c->precision, c->quad != 0, c->mask, walk_launch_grid(c), c->stream);
   launch_eval_done(c->st, c->stream);
 }
@@ -1383,10 +1393,10 @@ int bhg_get_stats(bhg_context* c, bhg_stats* out, int reset) {
   out->sort_passes = kSortPasses;
   // bounds + domain + keys + digit offsets; the sort passes; gather + roots +
   // one per level; the multipoles (one kernel, or one per level); mark +
-  // compact of the targets, packing + compact of the walk groups; walk + its
-  // completion count
-  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (c->n <= kMomentsOneLaunchMax ? 1 : kMortonDepth + 1) + 4 +
-                          2;
+  // compact of the targets, of the packing chunks, packing + compact of the
+  // walk groups; walk + its target pass + its completion count
+  out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (c->n <= kMomentsOneLaunchMax ? 1 : kMortonDepth + 1) + 6 +
+                          3;
   if (reset) {
     for (double& t : c->tot_ms) t = 0.0;
     c->walks_timed = 0;

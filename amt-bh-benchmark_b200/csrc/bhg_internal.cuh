@@ -101,6 +101,7 @@ struct DevState {
   uint32_t group_tiles;      // tiles taken by the group compaction
   uint32_t n_chunks;         // packing chunks of the walk groups
   uint32_t chunk_tiles;      // tiles taken by the chunk compaction
+  uint32_t walk_next2;       // next target of the walk's second pass
   unsigned long long pp, pc;  // interaction counts of the walk
 };
 constexpr size_t kBuildResetOffset = offsetof(DevState, n_nodes);

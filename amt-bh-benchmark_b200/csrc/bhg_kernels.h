@@ -58,9 +58,14 @@ struct WalkArgs {
   Particle* out;           // kicked/drifted particles (the state)
   double* accel;           // optional: G*a, 3 per particle
   DevState* st;
-  // per-warp lists of the sources only some targets of a group take
-  // (walk_list_cap() entries per warp of the grid)
+  // list slots (nslots, at least one per warp of the grid): the sources only
+  // some targets of a group take, per warp (one pass) or per group (two
+  // passes, when there are at most nslots groups); per slot also the group's
+  // FP64 sums (kGroupMax x 3) and list length
   uint2* wlist;
+  double* gsum;
+  uint32_t* gnl;
+  uint32_t nslots;
 };
 
 // Walks every target and kicks/drifts its particles.  precision:
@@ -68,8 +73,8 @@ struct WalkArgs {
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s);
 int walk_blocks_per_sm(int precision, bool quad, bool mask);
 int walk_threads();
-// entries of one warp's partial-source list
-size_t walk_list_cap();
+// device bytes of one list slot
+size_t walk_slot_bytes();
 
 void launch_integrate(Particle* p, const double* accel, uint32_t n, const SysDev* sys, const SysParam* prm, int nsys,
                       int sms, cudaStream_t s);

@@ -48,7 +48,8 @@ constexpr int kStageF4 = 3 * 64 + 3;  // staged source records (float4): 64 cell
 constexpr float kFarAway = 1.0e10f;  // padding source: contributes exactly 0
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kLeafBit = 0x80000000u;  // list entry: a leaf whose particles some targets take
-constexpr uint32_t kListCap = 8192;         // entries of one warp's partial-source list
+constexpr uint32_t kListCap = 4096;         // entries of one partial-source list (32 KB)
+constexpr uint32_t kNotShared = 0xffffffffu;  // a group whose list overflowed: its targets walk alone
 // a walk that pops one node at a time holds at most 7 entries per level
 // below the one it pops from, plus the root
 static_assert(kStackCap >= 7 * kLevels + 1 + 8, "a one-at-a-time walk must fit the stack");
@@ -758,7 +759,9 @@ __device__ __forceinline__ int group_walk(E& ev, const WalkArgs& a, WarpSmem& S,
 
 // Target `bit` of the group takes, from the list, the entries whose mask
 // holds it: cells into its cell queue, leaves' particles into its particle
-// queue; evaluated with the evaluator set up for its particles.
+// queue; evaluated with the evaluator set up for its particles.  The scan
+// moves a window of 32 entries at a time and skips windows without an entry
+// for the target.
 template <class E>
 __device__ __forceinline__ void target_pass(E& ev, const WalkArgs& a, WarpSmem& S, const uint2* list, uint32_t nlist,
                                             uint32_t bit, int lane, Queues& q) {
@@ -768,19 +771,25 @@ __device__ __forceinline__ void target_pass(E& ev, const WalkArgs& a, WarpSmem& 
   for (;;) {
     if (drain_step(ev, S, q, at < nlist, lane)) continue;
     if (at >= nlist) break;
-    const uint32_t j = at + (uint32_t)lane;
-    const uint2 e = j < nlist ? list[j] : make_uint2(0u, 0u);
-    const bool hit = (e.y >> bit) & 1u;
+    uint2 e;
+    bool hit;
+    do {
+      const uint32_t j = at + (uint32_t)lane;
+      e = j < nlist ? list[j] : make_uint2(0u, 0u);
+      hit = (e.y >> bit) & 1u;
+      at += 32;
+    } while (!__any_sync(kFull, hit) && at < nlist);
     const bool isleaf = (e.x & kLeafBit) != 0u;
-    push_cells(S, q, hit && !isleaf, e.x, lt);
-    uint32_t first = 0, cnt = 0;
-    if (hit && isleaf) {
-      const uint2 fc = *reinterpret_cast<const uint2*>(&a.w[e.x & ~kLeafBit].first);
-      first = fc.x, cnt = fc.y;
+    const bool chit = hit && !isleaf, lhit = hit && isleaf;
+    if (__any_sync(kFull, chit)) push_cells(S, q, chit, e.x, lt);
+    if (__any_sync(kFull, lhit)) {
+      uint32_t first = 0, cnt = 0;
+      if (lhit) {
+        const uint2 fc = *reinterpret_cast<const uint2*>(&a.w[e.x & ~kLeafBit].first);
+        first = fc.x, cnt = fc.y;
+      }
+      open_leaves(q, cnt, first, lane);
     }
-    open_leaves(q, cnt, first, lane);
-    at += 32;
-    __syncwarp();
   }
   __syncwarp();
 }
@@ -877,20 +886,44 @@ __device__ void targets_alone(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t ro
   }
 }
 
+// The group of walk group gi: its targets [t0, t1), first particle, system.
+struct GroupInfo {
+  uint32_t t0, t1, k, p0, s;
+};
+
+__device__ __forceinline__ GroupInfo group_info(const WalkArgs& a, uint32_t gi, uint32_t ngroups, uint32_t ntargets) {
+  GroupInfo g;
+  g.t0 = a.groups[gi];
+  g.t1 = gi + 1 < ngroups ? a.groups[gi + 1] : ntargets;
+  g.k = g.t1 - g.t0;
+  g.p0 = a.nbegin[a.targets[g.t0]];
+  g.s = a.nsys > 1 ? system_of(a, g.p0) : 0u;
+  return g;
+}
+
 // One warp per walk group (a run of targets, k_pack_groups).  A group of one
 // target larger than kGroupMax particles walks in batches of kGroupMax
 // targets.  Otherwise: the group's shared walk with every source all its
 // targets take evaluated against all its particles, then each target's pass
 // over the list of the sources only some take, each adding its part onto the
 // group's FP64 sums in target order; then the kick/drift.
+//
+// With few groups (n_groups <= a.nslots: about as many as warps, so the
+// largest group's targets would set the kernel's time) the work is cut in
+// two passes instead: this kernel runs the shared walks (and the groups of
+// one target whole) and leaves each group's FP64 sums and list in its own
+// slot; k_walk_targets then runs every target's pass as a job of its own.
+// Both schedules run the same passes and add each target's part onto the
+// group's sums the same way, so the results are the same bits.
 template <class E, bool QUAD>
 __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
   if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;  // the build failed: touch nothing
-  uint2* list = a.wlist + (size_t)(blockIdx.x * kWalkWarps + warp) * kListCap;
   const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
+  const bool two_pass = ngroups <= a.nslots;
+  const size_t wid = (size_t)blockIdx.x * kWalkWarps + warp;
   unsigned long long n_pp = 0, n_pc = 0;
   E ev(a, S.stage, lane);
   Queues q;
@@ -899,16 +932,13 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     if (lane == 0) gi = atomicAdd(&a.st->walk_next, 1u);
     gi = __shfl_sync(kFull, gi, 0);
     if (gi >= ngroups) break;
-    const uint32_t t0 = a.groups[gi], t1 = gi + 1 < ngroups ? a.groups[gi + 1] : ntargets;
-    const uint32_t k = t1 - t0;
-    const uint32_t first_node = a.targets[t0];
-    const uint32_t p0 = a.nbegin[first_node];
-    const uint32_t s = a.nsys > 1 ? system_of(a, p0) : 0u;
-    const uint32_t root = a.sys[s].root;
-    const SysParam& sp = a.prm[s];
+    const GroupInfo g = group_info(a, gi, ngroups, ntargets);
+    const uint32_t k = g.k, p0 = g.p0;
+    const uint32_t root = a.sys[g.s].root;
+    const SysParam& sp = a.prm[g.s];
     const double theta2 = sp.theta2;
-    ev.set_system(sp.eps2, a.sys[s].hw);
-    const uint32_t n0 = a.ncount[first_node];
+    ev.set_system(sp.eps2, a.sys[g.s].hw);
+    const uint32_t n0 = a.ncount[a.targets[g.t0]];
     if (k == 1 && n0 > (uint32_t)kGroupMax) {
       // a large target: batches of kGroupMax particles, each walking the
       // whole target's box from the root
@@ -934,7 +964,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     // the targets: particle ranges and boxes (lane i: target i), the group box
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     if ((uint32_t)lane < k) {
-      const uint32_t tn = a.targets[t0 + lane];
+      const uint32_t tn = a.targets[g.t0 + lane];
       const uint32_t tb = a.nbegin[tn], tc = a.ncount[tn];
       for (uint32_t i = 0; i < tc; ++i) {
         const double4 p = a.pm[tb + i];
@@ -962,6 +992,9 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     const uint32_t np = S.tbeg[k - 1] + S.tcnt[k - 1] - p0;
     for (uint32_t i = lane; i < np; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
     __syncwarp();
+    // the list: the warp's slot, or in the two-pass schedule the group's
+    const bool split = two_pass && k > 1;
+    uint2* list = a.wlist + (split ? (size_t)gi : wid) * kListCap;
     // the shared walk (redone one node at a time if the stack would overflow)
     ev.cx = 0.5 * (lo[0] + hi[0]), ev.cy = 0.5 * (lo[1] + hi[1]), ev.cz = 0.5 * (lo[2] + hi[2]);
     uint32_t nlist = 0;
@@ -974,6 +1007,17 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     if (r == 0) {
       ev.finish();
       add_counts(q, np, QUAD, n_pp, n_pc);
+    }
+    if (split) {  // the targets' passes run in k_walk_targets
+      if (r == 0) {
+        double* gs = a.gsum + (size_t)gi * (kGroupMax * 3);
+        for (uint32_t i = lane; i < np; i += 32) gs[3 * i] = S.acc[i][0], gs[3 * i + 1] = S.acc[i][1], gs[3 * i + 2] = S.acc[i][2];
+      }
+      if (lane == 0) a.gnl[gi] = r == 0 ? nlist : kNotShared;
+      __syncwarp();
+      continue;
+    }
+    if (r == 0) {
       // each target's part from the list, in target order
       if (nlist) {
         for (uint32_t i = 0; i < k; ++i) {
@@ -999,9 +1043,78 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   }
 }
 
+// The second pass of the two-pass schedule (see k_walk): one warp per target
+// of a group of more than one target: the group's FP64 sums for its
+// particles, then its pass over the group's list (or, if the list
+// overflowed, its own walk from the root), then the kick/drift.
+template <class E, bool QUAD>
+__global__ void __launch_bounds__(kWalkThreads, 4) k_walk_targets(WalkArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+  if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;
+  const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
+  if (ngroups > a.nslots) return;  // k_walk ran the one-pass schedule
+  unsigned long long n_pp = 0, n_pc = 0;
+  E ev(a, S.stage, lane);
+  Queues q;
+  for (;;) {
+    uint32_t ti = 0;
+    if (lane == 0) ti = atomicAdd(&a.st->walk_next2, 1u);
+    ti = __shfl_sync(kFull, ti, 0);
+    if (ti >= ntargets) break;
+    // its group: the last whose first target is at or before ti
+    uint32_t gi = 0, hi = ngroups;
+    while (hi - gi > 1) {
+      const uint32_t mid = (gi + hi) >> 1;
+      if (a.groups[mid] <= ti) gi = mid;
+      else hi = mid;
+    }
+    const GroupInfo g = group_info(a, gi, ngroups, ntargets);
+    if (g.k == 1) continue;  // done whole in the first pass
+    const uint32_t tnode = a.targets[ti];
+    const uint32_t tb = a.nbegin[tnode], tn = a.ncount[tnode];  // tn <= kGroupMax: inside a group
+    const uint32_t root = a.sys[g.s].root;
+    const SysParam& sp = a.prm[g.s];
+    ev.set_system(sp.eps2, a.sys[g.s].hw);
+    double lo[3], hi3[3];
+    particle_box(a.pm, tb, tn, lane, lo, hi3);
+    ev.cx = 0.5 * (lo[0] + hi3[0]), ev.cy = 0.5 * (lo[1] + hi3[1]), ev.cz = 0.5 * (lo[2] + hi3[2]);
+    const uint32_t nlist = a.gnl[gi];
+    if (nlist == kNotShared) {
+      for (uint32_t i = lane; i < tn; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
+      __syncwarp();
+      int r = 0;
+      for (int attempt = 0; attempt < 2; ++attempt) {
+        ev.setup(lane, tb, (int)tn, S.acc);
+        r = target_walk(ev, a, S, root, lo, hi3, sp.theta2, attempt == 1, lane, q);
+        if (r == 0) break;
+      }
+      ev.finish();
+      add_counts(q, tn, QUAD, n_pp, n_pc);
+    } else {
+      const double* gs = a.gsum + (size_t)gi * (kGroupMax * 3) + 3 * (size_t)(tb - g.p0);
+      for (uint32_t i = lane; i < tn; i += 32) S.acc[i][0] = gs[3 * i], S.acc[i][1] = gs[3 * i + 1], S.acc[i][2] = gs[3 * i + 2];
+      __syncwarp();
+      if (nlist) {
+        ev.setup(lane, tb, (int)tn, S.acc);
+        target_pass(ev, a, S, a.wlist + (size_t)gi * kListCap, nlist, ti - g.t0, lane, q);
+        ev.finish();
+        add_counts(q, tn, QUAD, n_pp, n_pc);
+      }
+    }
+    kick_drift(a, sp, S.acc, tb, tn, lane);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.st->pp, n_pp);
+    atomicAdd(&a.st->pc, n_pc);
+  }
+}
+
 template <class E, bool QUAD>
 static void launch_one(const WalkArgs& a, int grid, cudaStream_t s) {
   k_walk<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
+  k_walk_targets<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
 }
 
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s) {
@@ -1017,6 +1130,7 @@ void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int gri
 template <class E, bool QUAD>
 static int occ() {
   cudaFuncSetAttribute(k_walk<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
+  cudaFuncSetAttribute(k_walk_targets<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
   int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<E, QUAD>, kWalkThreads, kWalkSmem);
   return b > 0 ? b : 1;
@@ -1042,7 +1156,9 @@ int walk_blocks_per_sm(int precision, bool quad, bool mask) {
 
 int walk_threads() { return kWalkThreads; }
 
-size_t walk_list_cap() { return kListCap; }
+// Device bytes of one list slot: the list, and the group's FP64 sums and
+// list length for the two-pass schedule.
+size_t walk_slot_bytes() { return kListCap * sizeof(uint2) + kGroupMax * 3 * sizeof(double) + sizeof(uint32_t); }
 
 // ---------------------------------------------------------------------------
 // Unfused integrate phase: kick_one / drift_one (integrate.h:15-16) with

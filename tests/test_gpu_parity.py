@@ -195,19 +195,23 @@ def test_walk_group_sizes_match_oracle(gpu, oracle, precision, tol, group):
 
 
 @pytest.mark.parametrize("precision", [bhg.PRECISION_SPLIT, bhg.PRECISION_FP64])
-def test_budget_limited_walk_grid_same_bits(precision):
-    """Under a tight HBM budget the walk runs on fewer blocks (as many as
-    have their lists within the budget): the same bits as on the full grid."""
+def test_two_pass_walk_equals_one_pass(precision):
+    """About 550 walk groups: with the full set of list slots (two per warp)
+    the walk runs its two-pass schedule (shared walks, then every target's
+    pass as a job of its own); under a 20 MB budget there is room for ~260
+    slots only, so it runs one warp per group on fewer blocks.  Same bits."""
     parts = bhg.plummer(30000, 31)[0]
     fp = bhg.Context.params(0.5, 1e-4, 1.0, True, precision)
-    out = {}
-    for budget in (0, 40 << 20):
+    out, stats = {}, {}
+    for budget in (0, 20 << 20):
         with bhg.Context(device=0, hbm_budget=budget) as ctx:
             ctx.upload(parts)
             for _ in range(2):
                 ctx.step(fp, 16, 256, 16, 0.01, 0.01)
             out[budget] = ctx.download()
-    assert out[0].tobytes() == out[40 << 20].tobytes()
+            stats[budget] = ctx.stats()
+    assert (stats[0]["pp"], stats[0]["pc"]) == (stats[20 << 20]["pp"], stats[20 << 20]["pc"])
+    assert out[0].tobytes() == out[20 << 20].tobytes()
 
 
 def test_no_softening_masks_self(gpu, oracle):
