@@ -148,6 +148,6 @@ constexpr uint32_t kNoParent = 0xffffffffu;
 constexpr int kTile = 4096;  // particles per radix-sort / bounds tile
 constexpr int kSortPasses = 8;
 constexpr int kGroupMax = 64;    // particles of a walk group (targets sharing one traversal)
-constexpr int kMaxTargets = 32;  // targets of a walk group (the bits of a traversal mask)
+constexpr int kMaxTargets = 24;  // targets of a walk group (the bits of a traversal mask)
 
 }  // namespace bhg

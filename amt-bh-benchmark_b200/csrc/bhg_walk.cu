@@ -47,7 +47,14 @@ constexpr int kStackCap = 704;   // per-warp stack: node + target mask per entry
 constexpr int kStageF4 = 3 * 64 + 3;  // staged source records (float4): 64 cells + the zero cell
 constexpr float kFarAway = 1.0e10f;  // padding source: contributes exactly 0
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kLeafBit = 0x80000000u;  // list entry: a leaf whose particles some targets take
+// A list entry is (node, target mask) for a cell, or (first particle |
+// kLeafBit, target mask | count << kCountShift) for a run of at most
+// kMaxRun particles of a leaf (a larger leaf takes several entries), so that
+// the targets' passes need no second load for it.
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr int kCountShift = 24;
+constexpr uint32_t kMaxRun = 255;
+static_assert(kMaxTargets <= kCountShift, "target masks and run lengths share a word");
 constexpr uint32_t kListCap = 4096;         // entries of one partial-source list (32 KB)
 constexpr uint32_t kNotShared = 0xffffffffu;  // a group whose list overflowed: its targets walk alone
 // a walk that pops one node at a time holds at most 7 entries per level
@@ -655,7 +662,7 @@ template <class E>
 __device__ __forceinline__ int group_walk(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t root, uint32_t k,
                                           double theta2, bool dfs, int lane, uint2* list, uint32_t& nlist, Queues& q) {
   const uint32_t lt = lanemask_lt();
-  const uint32_t full = k == 32 ? kFull : ((1u << k) - 1u);
+  const uint32_t full = (1u << k) - 1u;  // k <= kMaxTargets < 32
   if (lane == 0) S.snode[0] = root, S.smask[0] = full;
   uint32_t top = 1;
   __syncwarp();
@@ -734,13 +741,17 @@ __device__ __forceinline__ int group_walk(E& ev, const WalkArgs& a, WarpSmem& S,
     push_cells(S, q, A != 0u && A == full, node, lt);
     // sources some targets take: the list
     const bool cpart = A != 0u && A != full, lpart = leaf && O != 0u && O != full;
-    const uint32_t nl = (cpart ? 1u : 0u) + (lpart ? 1u : 0u);
+    const uint32_t runs = lpart ? (u4.y + kMaxRun - 1) / kMaxRun : 0u;
+    const uint32_t nl = (cpart ? 1u : 0u) + runs;
     const uint32_t linc = warp_incl_scan_u32(nl, lane);
     const uint32_t ltot = __shfl_sync(kFull, linc, 31);
     if (nlist + ltot > kListCap) return 2;
     uint32_t at = nlist + linc - nl;
     if (cpart) list[at++] = make_uint2(node, A);
-    if (lpart) list[at] = make_uint2(node | kLeafBit, O);
+    for (uint32_t r = 0; r < runs; ++r) {
+      const uint32_t c = min(kMaxRun, u4.y - r * kMaxRun);
+      list[at++] = make_uint2((u4.x + r * kMaxRun) | kLeafBit, O | (c << kCountShift));
+    }
     nlist += ltot;
     // opened interior nodes: children, with the targets that opened them
     const uint32_t nch = (O != 0u && !leaf) ? info_nchild(u4.z) : 0u;
@@ -768,28 +779,25 @@ __device__ __forceinline__ void target_pass(E& ev, const WalkArgs& a, WarpSmem& 
   const uint32_t lt = lanemask_lt();
   q = Queues();
   uint32_t at = 0;
+  // the window after `at` is loaded one window ahead, so that its load
+  // overlaps the work on the current one
+  uint2 next = (uint32_t)lane < nlist ? list[lane] : make_uint2(0u, 0u);
   for (;;) {
     if (drain_step(ev, S, q, at < nlist, lane)) continue;
     if (at >= nlist) break;
     uint2 e;
     bool hit;
     do {
-      const uint32_t j = at + (uint32_t)lane;
-      e = j < nlist ? list[j] : make_uint2(0u, 0u);
+      e = next;
       hit = (e.y >> bit) & 1u;
       at += 32;
+      const uint32_t j = at + (uint32_t)lane;
+      next = j < nlist ? list[j] : make_uint2(0u, 0u);
     } while (!__any_sync(kFull, hit) && at < nlist);
     const bool isleaf = (e.x & kLeafBit) != 0u;
     const bool chit = hit && !isleaf, lhit = hit && isleaf;
     if (__any_sync(kFull, chit)) push_cells(S, q, chit, e.x, lt);
-    if (__any_sync(kFull, lhit)) {
-      uint32_t first = 0, cnt = 0;
-      if (lhit) {
-        const uint2 fc = *reinterpret_cast<const uint2*>(&a.w[e.x & ~kLeafBit].first);
-        first = fc.x, cnt = fc.y;
-      }
-      open_leaves(q, cnt, first, lane);
-    }
+    if (__any_sync(kFull, lhit)) open_leaves(q, lhit ? e.y >> kCountShift : 0u, e.x & ~kLeafBit, lane);
   }
   __syncwarp();
 }

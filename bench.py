@@ -96,6 +96,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="ensemble: skip the one-at-a-time FP64 path")
+    ap.add_argument("--walk-group", type=int, default=0,
+                    help="single systems: walk-group particle cap (0 = the library's default)")
     ap.add_argument("--no-north-star", action="store_true",
                     help="plummer-4m: skip the ensemble and serving gates run after the main measurement")
     ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
@@ -523,6 +525,7 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     fp = bhg.Context.params(w["theta"], w["eps"] ** 2, 1.0, True, prec)
     ctx = bhg.Context(device=rig.local)
     ctx.set_stream(rig.stream.cuda_stream)
+    ctx.set_walk_shape(args.walk_group)
     ctx.upload(parts)
 
     def one_step():
@@ -558,7 +561,7 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     ctx.close()
     if rig.rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_single(w)
-    out["config_extra"] = {"n": n}
+    out["config_extra"] = {"n": n, "walk_group": args.walk_group or 64}
     return out
 
 
