@@ -523,9 +523,18 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     n = len(parts)
     prec = bhg.PRECISION_SPLIT if args.precision == "split" else bhg.PRECISION_FP64
     fp = bhg.Context.params(w["theta"], w["eps"] ** 2, 1.0, True, prec)
+    walk_group, tuned = args.walk_group, None
+    if not walk_group:
+        # the walk-group cap from the autotuner (leaf and target sizes are the
+        # workload's own; theta is never tuned)
+        from bhg import autotune
+
+        tuned = autotune.tune([parts], w["theta"], w["eps"] ** 2, w["group"], prec, device=rig.local,
+                              cands=autotune.candidates(leaves=(w["max_leaf"],), walk_groups=(32, 64)))
+        walk_group = tuned["walk_group"]
     ctx = bhg.Context(device=rig.local)
     ctx.set_stream(rig.stream.cuda_stream)
-    ctx.set_walk_shape(args.walk_group)
+    ctx.set_walk_shape(walk_group)
     ctx.upload(parts)
 
     def one_step():
@@ -561,7 +570,9 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
     ctx.close()
     if rig.rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_single(w)
-    out["config_extra"] = {"n": n, "walk_group": args.walk_group or 64}
+    out["config_extra"] = {"n": n, "walk_group": walk_group}
+    if tuned is not None:
+        out["autotune"] = {k: tuned[k] for k in ("walk_group", "rms_error", "err_budget", "table")}
     return out
 
 
@@ -650,6 +661,10 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
         ctxs = []
         for p in systems:
             c = bhg.Context(device=rig.local)
+            # one system per context: below 131,072 particles the smaller
+            # walk groups keep more warps busy (plummer-65k: 0.63 ms walk at
+            # 32 against 0.85 ms at 64)
+            c.set_walk_shape(32 if len(p) < 131072 else 64)
             c.upload(p)
             ctxs.append(c)
 
@@ -669,7 +684,8 @@ def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
         pv = ps / (pms / 1000.0)
         out["plain_fp64_one_at_a_time"] = {
             "value": pv, "unit": "particle-steps/s", "ms_per_step": pms / args.steps,
-            "path": "512 resident contexts stepped in turn, FP64 walk, leaf/target 16, group 256 (wall clock)"}
+            "path": "512 resident contexts stepped in turn, FP64 walk, leaf/target 16, group 256, walk groups of "
+                    "32 particles below 131,072 particles and 64 above (wall clock)"}
         out["speedup_vs_plain"] = out["value"] / pv
 
     if rig.rank == 0 and not args.no_cpu_baseline:
