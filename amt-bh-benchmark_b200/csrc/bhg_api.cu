@@ -94,9 +94,14 @@ struct bhg_context {
   int async_pending = 0;
   uint32_t async_base = 0;
 
-  // captured graphs, one per phase
-  cudaGraphExec_t graph[kPhases] = {};
-  std::string graph_key[kPhases];
+  // one evaluation (every phase) captured as one graph; its phase-boundary
+  // events are event-record nodes, pointed at fresh events before each
+  // launch (cap_ev: the placeholders recorded during capture)
+  cudaGraph_t step_graph = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  std::string step_key;
+  cudaGraphNode_t step_ev_node[kPhases + 1] = {};
+  cudaEvent_t cap_ev[kPhases + 1] = {};
 };
 
 namespace {
@@ -148,11 +153,11 @@ int grow(bhg_context* c, T** p, size_t count) {
 }
 
 void drop_graph(bhg_context* c) {
-  for (int p = 0; p < kPhases; ++p) {
-    if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
-    c->graph[p] = nullptr;
-    c->graph_key[p].clear();
-  }
+  if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
+  if (c->step_graph) cudaGraphDestroy(c->step_graph);
+  c->step_exec = nullptr;
+  c->step_graph = nullptr;
+  c->step_key.clear();
 }
 
 // Device bytes of one node slot (the SoA arrays, the walk record, the cut
@@ -273,7 +278,10 @@ int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles, size_t n
 constexpr uint32_t kSmallSortTile = 1024;
 constexpr size_t kSmallSortMax = 196608;
 
-uint32_t sort_tile_keys(size_t n) { return n <= kSmallSortMax ? kSmallSortTile : (uint32_t)kTile; }
+#ifndef BHG_LARGE_SORT_TILE
+#define BHG_LARGE_SORT_TILE kTile
+#endif
+uint32_t sort_tile_keys(size_t n) { return n <= kSmallSortMax ? kSmallSortTile : (uint32_t)BHG_LARGE_SORT_TILE; }
 
 // Tiles of `tile` particles over systems of the given sizes.
 size_t count_tiles(const std::vector<uint64_t>& counts, uint32_t tile) {
@@ -519,8 +527,8 @@ void fold_times(bhg_context* c) {
   c->open_ev = nullptr;
 }
 
-// Runs `enq` as phase `phase`: from a captured graph when `graphed`, with a
-// CUDA event before and after it on the stream.
+// Runs `enq` as phase `phase`, with a CUDA event before and after it on the
+// stream (the per-phase calls; a whole evaluation runs as one graph, enq_step).
 // NVTX range names of the phases (host-side enqueue ranges; a profiler shows
 // the kernels under them)
 const char* const kPhaseName[kPhases] = {"bhg pre", "bhg sort", "bhg tree", "bhg moments", "bhg targets", "bhg walk"};
@@ -531,7 +539,7 @@ struct NvtxRange {
 };
 
 template <typename F>
-int run_phase(bhg_context* c, int phase, bool graphed, const std::string& key, F enq) {
+int run_phase(bhg_context* c, int phase, F enq) {
   const NvtxRange range(kPhaseName[phase]);
   if (c->pending.size() > 16384) fold_times(c);
   if (!c->open_ev) {
@@ -539,27 +547,8 @@ int run_phase(bhg_context* c, int phase, bool graphed, const std::string& key, F
     CK(cudaEventRecord(c->open_ev, c->stream));
   }
   cudaEvent_t a = c->open_ev;
-  if (graphed) {
-    if (!c->graph[phase] || c->graph_key[phase] != key) {
-      if (c->graph[phase]) cudaGraphExecDestroy(c->graph[phase]);
-      c->graph[phase] = nullptr;
-      cudaGraph_t g = nullptr;
-      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      enq();
-      CK(cudaStreamEndCapture(c->stream, &g));
-      cudaError_t e = cudaGraphInstantiate(&c->graph[phase], g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) {
-        c->graph[phase] = nullptr;
-        return fail(c, BHG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      }
-      c->graph_key[phase] = key;
-    }
-    CK(cudaGraphLaunch(c->graph[phase], c->stream));
-  } else {
-    enq();
-    CK(cudaGetLastError());
-  }
+  enq();
+  CK(cudaGetLastError());
   cudaEvent_t b = take_event(c);
   CK(cudaEventRecord(b, c->stream));
   c->pending.push_back({phase, a, b});
@@ -575,11 +564,10 @@ std::string graph_key(const bhg_context* c, uint32_t target_size) {
 }
 
 // The three build phases (bhg_build_tree).
-int run_build(bhg_context* c, bool graphed, const std::string& key) {
+int run_build(bhg_context* c) {
   int r;
-  if ((r = run_phase(c, kPre, graphed, key, [&] { enq_pre(c); })) ||
-      (r = run_phase(c, kSort, graphed, key, [&] { enq_sort(c); })) ||
-      (r = run_phase(c, kTree, graphed, key, [&] { enq_tree(c); })))
+  if ((r = run_phase(c, kPre, [&] { enq_pre(c); })) || (r = run_phase(c, kSort, [&] { enq_sort(c); })) ||
+      (r = run_phase(c, kTree, [&] { enq_tree(c); })))
     return r;
   return BHG_OK;
 }
@@ -683,6 +671,7 @@ int bhg_create(bhg_context** out, const bhg_config* cfg) {
     return BHG_ENOMEM;
   }
   cudaMemsetAsync(c->st, 0, sizeof(DevState), c->stream);
+  std::memset(c->st_host, 0, sizeof(DevState));  // the host's copy of the (zero) device state
   *out = c;
   return BHG_OK;
 }
@@ -696,6 +685,8 @@ int bhg_destroy(bhg_context* c) {
   c->allocs.clear();
   if (c->st_host) cudaFreeHost(c->st_host);
   for (auto& ev : c->ev_all)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->cap_ev)
     if (ev) cudaEventDestroy(ev);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1127,7 +1118,7 @@ int bhg_build_tree(bhg_context* c, unsigned max_leaf, uint32_t group_size) {
   c->group_size = group_size;
   if ((r = ensure_nodes(c, node_estimate(c->n, c->nsys, max_leaf)))) return r;
   for (int attempt = 0; attempt < 8; ++attempt) {
-    if ((r = run_build(c, false, ""))) return r;
+    if ((r = run_build(c))) return r;
     if ((r = read_state(c))) return r;
     if (c->st_host->status & kStNodeOverflow) {
       size_t need = std::max<size_t>(2 * c->cap_nodes, (size_t)c->st_host->n_nodes + c->st_host->n_nodes / 4 + 64);
@@ -1149,7 +1140,7 @@ int bhg_compute_multipoles(bhg_context* c) {
   if (!c) return BHG_EINVAL;
   if (!c->built) return fail(c, BHG_ESTATE, "build the tree first");
   cudaSetDevice(c->device);
-  int r = run_phase(c, kMoments, false, "", [&] { enq_moments(c); });
+  int r = run_phase(c, kMoments, [&] { enq_moments(c); });
   if (r) return r;
   c->moments = true;
   return BHG_OK;
@@ -1164,8 +1155,8 @@ int bhg_walk_forces(bhg_context* c, const bhg_force_params* fp, uint32_t target_
   if (r) return r;
   if (!c->accel && (r = grow(c, &c->accel, c->cap_n * 3))) return r;
   if ((r = ensure_walk_scratch(c, walk_grid(c))) || (r = push_params(c))) return r;
-  if ((r = run_phase(c, kTargets, false, "", [&] { enq_targets(c, target_size); })) ||
-      (r = run_phase(c, kWalk, false, "", [&] { enq_walk(c, true); })))
+  if ((r = run_phase(c, kTargets, [&] { enq_targets(c, target_size); })) ||
+      (r = run_phase(c, kWalk, [&] { enq_walk(c, true); })))
     return r;
   c->walked = true;
   c->moments = false;  // the state moved: the next walk needs a new build
@@ -1215,15 +1206,74 @@ int bhg_set_system_params(bhg_context* c, const double* theta, const double* eps
 
 namespace {
 
-// One whole evaluation (build + multipoles + walk), each phase replayed from
-// its captured graph.
+// One whole evaluation (build + multipoles + targets + walk) as ONE graph
+// launch: captured once per problem shape, replayed after.  An event-record
+// node sits at every phase boundary; before each launch they are pointed at
+// fresh events (cudaGraphExecEventRecordNodeSetEvent, which leaves launches
+// already in flight alone), so the phase times of every evaluation are still
+// CUDA-event times on the context's stream.
 int enq_step(bhg_context* c, uint32_t target_size) {
+  const NvtxRange range("bhg step");
   const std::string key = graph_key(c, target_size);
-  int r;
-  if ((r = run_build(c, true, key)) || (r = run_phase(c, kMoments, true, key, [&] { enq_moments(c); })) ||
-      (r = run_phase(c, kTargets, true, key, [&] { enq_targets(c, target_size); })) ||
-      (r = run_phase(c, kWalk, true, key, [&] { enq_walk(c, false); })))
-    return r;
+  if (c->pending.size() > 16384) fold_times(c);
+  if (!c->step_exec || c->step_key != key) {
+    drop_graph(c);
+    for (int i = 0; i <= kPhases; ++i)
+      if (!c->cap_ev[i]) CK(cudaEventCreate(&c->cap_ev[i]));
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecordWithFlags(c->cap_ev[kPre], c->stream, cudaEventRecordExternal);
+    enq_pre(c);
+    cudaEventRecordWithFlags(c->cap_ev[kSort], c->stream, cudaEventRecordExternal);
+    enq_sort(c);
+    cudaEventRecordWithFlags(c->cap_ev[kTree], c->stream, cudaEventRecordExternal);
+    enq_tree(c);
+    cudaEventRecordWithFlags(c->cap_ev[kMoments], c->stream, cudaEventRecordExternal);
+    enq_moments(c);
+    cudaEventRecordWithFlags(c->cap_ev[kTargets], c->stream, cudaEventRecordExternal);
+    enq_targets(c, target_size);
+    cudaEventRecordWithFlags(c->cap_ev[kWalk], c->stream, cudaEventRecordExternal);
+    enq_walk(c, false);
+    cudaEventRecordWithFlags(c->cap_ev[kPhases], c->stream, cudaEventRecordExternal);
+    CK(cudaStreamEndCapture(c->stream, &g));
+    // the event-record nodes (recorded as external events, so that capture
+    // turns them into nodes), known by the placeholder event each records
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    for (int i = 0; i <= kPhases; ++i) c->step_ev_node[i] = nullptr;
+    for (cudaGraphNode_t node : nodes) {
+      cudaGraphNodeType t;
+      CK(cudaGraphNodeGetType(node, &t));
+      if (t != cudaGraphNodeTypeEventRecord) continue;
+      cudaEvent_t e = nullptr;
+      CK(cudaGraphEventRecordNodeGetEvent(node, &e));
+      for (int i = 0; i <= kPhases; ++i)
+        if (e == c->cap_ev[i]) c->step_ev_node[i] = node;
+    }
+    for (int i = 0; i <= kPhases; ++i)
+      if (!c->step_ev_node[i]) {
+        cudaGraphDestroy(g);
+        return fail(c, BHG_ECUDA, "captured evaluation graph lacks a phase event");
+      }
+    cudaError_t e = cudaGraphInstantiate(&c->step_exec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      c->step_exec = nullptr;
+      return fail(c, BHG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    c->step_graph = g;
+    c->step_key = key;
+  }
+  cudaEvent_t ev[kPhases + 1];
+  for (int i = 0; i <= kPhases; ++i) {
+    ev[i] = take_event(c);
+    CK(cudaGraphExecEventRecordNodeSetEvent(c->step_exec, c->step_ev_node[i], ev[i]));
+  }
+  CK(cudaGraphLaunch(c->step_exec, c->stream));
+  for (int p = 0; p < kPhases; ++p) c->pending.push_back({p, ev[p], ev[p + 1]});
+  c->open_ev = ev[kPhases];
   return BHG_OK;
 }
 
@@ -1279,8 +1329,10 @@ int run_evals(bhg_context* c, uint32_t target_size, const std::vector<std::pair<
   size_t next = 0;
   for (int attempt = 0; attempt < 8; ++attempt) {
     int r;
-    if ((r = read_state(c))) return r;
-    if (c->async_pending && (r = finish_async(c))) return r;
+    // the host's copy of the device state is current unless asynchronous
+    // evaluations are still out (every other path that runs a walk ends by
+    // reading it): no blocking read before the evaluations are enqueued
+    if (c->async_pending && ((r = read_state(c)) || (r = finish_async(c)))) return r;
     const uint32_t base = c->st_host->evals_ok;
     for (size_t i = next; i < kd.size(); ++i) {
       if (!keep) {
