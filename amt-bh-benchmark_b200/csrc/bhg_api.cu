@@ -278,10 +278,7 @@ int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles, size_t n
 constexpr uint32_t kSmallSortTile = 1024;
 constexpr size_t kSmallSortMax = 196608;
 
-#ifndef BHG_LARGE_SORT_TILE
-#define BHG_LARGE_SORT_TILE kTile
-#endif
-uint32_t sort_tile_keys(size_t n) { return n <= kSmallSortMax ? kSmallSortTile : (uint32_t)BHG_LARGE_SORT_TILE; }
+uint32_t sort_tile_keys(size_t n) { return n <= kSmallSortMax ? kSmallSortTile : (uint32_t)kTile; }
 
 // Tiles of `tile` particles over systems of the given sizes.
 size_t count_tiles(const std::vector<uint64_t>& counts, uint32_t tile) {

@@ -790,7 +790,6 @@ void set_build_attributes() {
   if (done) return;
   cudaFuncSetAttribute(k_sort_pass<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem<16>());
   cudaFuncSetAttribute(k_sort_pass<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem<4>());
-  cudaFuncSetAttribute(k_sort_pass<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem<8>());
   done = true;
 }
 
@@ -811,8 +810,6 @@ void launch_sort_pass(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, 
                       DevState* st, cudaStream_t s) {
   if (tile_keys == kSortThreads * 4)
     k_sort_pass<4><<<ntiles, kSortThreads, sort_smem<4>(), s>>>(kin, vin, kout, vout, pass, tiles, offs, lookback, st);
-  else if (tile_keys == kSortThreads * 8)
-    k_sort_pass<8><<<ntiles, kSortThreads, sort_smem<8>(), s>>>(kin, vin, kout, vout, pass, tiles, offs, lookback, st);
   else
     k_sort_pass<16><<<ntiles, kSortThreads, sort_smem<16>(), s>>>(kin, vin, kout, vout, pass, tiles, offs, lookback, st);
 }

@@ -959,7 +959,9 @@ def main():
     else:
         res = bench_single(args, w, rig, bhg, fp32_peak, peaks)
         dtype = "f32+f64" if args.precision == "split" else "f64"
-    if w["kind"] == "single" and args.workload == "plummer-4m" and not args.no_north_star:
+    # the gates are single-GPU ones: not repeated on every replica of a
+    # multi-GPU run
+    if w["kind"] == "single" and args.workload == "plummer-4m" and not args.no_north_star and rig.world == 1:
         res["north_star"] = north_star_block(args, rig, bhg, fp32_peak, peaks)
     if rig.rank == 0:
         cfg = workload_config(args.workload, w, rig.world)
