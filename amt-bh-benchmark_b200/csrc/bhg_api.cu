@@ -40,7 +40,7 @@ struct bhg_context {
   std::vector<SysParam> prm_host;
   std::vector<Tile> tiles_host;   // bounds/keys tiles (kTile particles)
   std::vector<Tile> stiles_host;  // radix-sort tiles (sort_tile keys)
-  uint32_t sort_tile = kTile;
+  uint32_t sort_tile = kSortTileLarge;
   std::vector<std::pair<void*, size_t>> allocs;
 
   // capacities (cap_n covers the scratch, cap_part the state; a capacity is
@@ -271,14 +271,13 @@ int ensure_particles(bhg_context* c, size_t n, int nsys, size_t ntiles, size_t n
   return BHG_OK;
 }
 
-// Keys per radix-sort tile: kSmallSortTile up to kSmallSortMax particles in
+// Keys per radix-sort tile: kSortTileSmall up to kSmallSortMax particles in
 // the context (four times the blocks per pass where there are few tiles),
-// kTile above.  Measured per evaluation (4096- / 1024-key tiles): 1.034 /
+// kSortTileLarge above.  Measured per evaluation (4096- / 1024-key tiles): 1.034 /
 // 1.037 ms at 65k, 1.633 / 1.559 at 131k, 2.755 / 2.792 at 262k.
-constexpr uint32_t kSmallSortTile = 1024;
 constexpr size_t kSmallSortMax = 196608;
 
-uint32_t sort_tile_keys(size_t n) { return n <= kSmallSortMax ? kSmallSortTile : (uint32_t)kTile; }
+uint32_t sort_tile_keys(size_t n) { return n <= kSmallSortMax ? kSortTileSmall : kSortTileLarge; }
 
 // Tiles of `tile` particles over systems of the given sizes.
 size_t count_tiles(const std::vector<uint64_t>& counts, uint32_t tile) {
@@ -791,7 +790,7 @@ int bhg_reserve(bhg_context* c, size_t particles, size_t systems) {
   const size_t n = std::max(particles, c->n);
   const size_t nsys = std::max(systems, c->counts.size());
   int r;
-  const size_t nst = std::max(n / kTile, std::min(n, kSmallSortMax) / kSmallSortTile) + nsys;
+  const size_t nst = std::max(n / kSortTileLarge, std::min(n, kSmallSortMax) / kSortTileSmall) + nsys;
   if ((r = ensure_particles(c, n, (int)nsys, n / kTile + nsys, nst)) || (r = ensure_nodes(c, node_estimate(n, (int)nsys, 16))))
     return r;
   return BHG_OK;

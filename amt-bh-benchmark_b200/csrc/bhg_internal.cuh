@@ -145,7 +145,9 @@ struct Nodes {
 constexpr uint32_t kNoParent = 0xffffffffu;
 
 // Kernel-launch helpers shared by the .cu files (defined in bhg_build.cu).
-constexpr int kTile = 4096;  // particles per radix-sort / bounds tile
+constexpr int kTile = 4096;  // particles per bounds / keys tile
+// keys per radix-sort tile: small problems, the rest
+constexpr int kSortTileSmall = 1024, kSortTileLarge = 4096;
 constexpr int kSortPasses = 8;
 constexpr int kGroupMax = 64;    // particles of a walk group (targets sharing one traversal)
 constexpr int kMaxTargets = 24;  // targets of a walk group (the bits of a traversal mask)
