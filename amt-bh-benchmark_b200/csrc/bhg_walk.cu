@@ -11,21 +11,25 @@
 // leaf included (its self term is 0 with softening and masked at r^2 = 0
 // without, accumulate_list grouped_ttg.h:117-163).
 //
-// One warp per walk GROUP (the topmost nodes with at most kGroupMax
-// particles, or leaves), sharing the upper walk among the group's targets as
-// GroupWalker::visit does: a first walk with the group's bounding box
-// resolves every node that is accepted for the whole box (then accepted for
-// every target inside it) or rejected for every point of it (mac_reject_all,
-// multipole.h:158-160: then opened by every target), evaluating those
-// interactions once against all of the group's particles; the rest is
-// deferred, and each target then walks only from the deferred nodes.  Each
-// target's list is the same as a separate walk from the root would build.
+// One warp per walk GROUP (a run of consecutive targets of one system, at
+// most kGroupMax particles and kMaxTargets targets, k_pack_groups), sharing
+// the walk among the group's targets as GroupWalker::visit does, taken to
+// every level: one traversal from the root whose stack entries carry the
+// mask of targets that still need the node.  A node accepted for the
+// group's bounding box is accepted by every target in the mask; one rejected
+// for every point of it (mac_reject_all, multipole.h:158-160) is opened by
+// all of them; otherwise each target in the mask tests its own box, one
+// (node, target) pair per lane.  Sources every target of the group takes are
+// evaluated once against all the group's particles; sources only some take
+// go to the warp's list as (node or leaf run, target mask), and each target
+// then passes over the list taking its own entries.  Each target's list is
+// the same as a separate walk of its box from the root would build.
 //
-// A walk step pops up to 32 nodes (one per lane) from a shared-memory stack;
-// accepted cells and opened leaves' particles go to two shared-memory
-// queues, and a full queue is evaluated as one batch (64 cells or 192
-// particles in split precision; one source per lane against up to 2 targets
-// per lane in FP64).
+// A walk step pops up to 32 entries (one per lane) from a shared-memory
+// stack; accepted cells and opened leaves' particles go to two
+// shared-memory queues, and a full queue is evaluated as one batch (64 cells
+// or 192 particles in split precision; one source per lane against up to 2
+// targets per lane in FP64).
 //
 // Split precision: sources and targets become FP32 offsets from the walk's
 // bounding-box centre (the subtraction in FP64), staged once per batch in
