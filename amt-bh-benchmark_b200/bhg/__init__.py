@@ -25,7 +25,7 @@ PARTICLE = np.dtype(
 
 OK, EINVAL, ECUDA, ENOMEM, ENONFINITE, ESTATE, EDEVICE, ECANCELLED, EAGAIN = range(9)
 PRECISION_SPLIT, PRECISION_FP64 = 0, 1
-EXPORT_KEYS, EXPORT_PERM, EXPORT_NODES_U32, EXPORT_NODES_F64, EXPORT_DOMAINS, EXPORT_TARGETS, EXPORT_ACCEL = range(1, 8)
+EXPORT_KEYS, EXPORT_PERM, EXPORT_NODES_U32, EXPORT_NODES_F64, EXPORT_DOMAINS, EXPORT_TARGETS, EXPORT_ACCEL, EXPORT_GROUPS = range(1, 9)
 
 #: Every entry point include/bhg.h declares.
 EXPORTED = (
@@ -394,7 +394,7 @@ class Context:
         self._ck(self.L.bhg_debug_export(self.h, what, _p(buf), size.value, C.byref(size)))
         if what == EXPORT_KEYS:
             return buf.view(np.uint64)
-        if what in (EXPORT_PERM, EXPORT_TARGETS):
+        if what in (EXPORT_PERM, EXPORT_TARGETS, EXPORT_GROUPS):
             return buf.view(np.uint32)
         if what == EXPORT_NODES_U32:
             u = buf.view(np.uint32).reshape(6, -1)

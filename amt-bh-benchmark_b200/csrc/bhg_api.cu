@@ -1527,6 +1527,10 @@ int bhg_debug_export(bhg_context* c, int what, void* out, size_t bytes, size_t* 
       buf.resize((size_t)c->st_host->n_targets * 4);
       if ((r = get(c->targets, buf.size(), 0))) return r;
       break;
+    case BHG_EXPORT_GROUPS:
+      buf.resize((size_t)c->st_host->n_groups * 4);
+      if ((r = get(c->groups, buf.size(), 0))) return r;
+      break;
     case BHG_EXPORT_ACCEL:
       if (!c->accel) return fail(c, BHG_ESTATE, "no accelerations stored (bhg_walk_forces stores them)");
       buf.resize(c->n * 24);

@@ -670,6 +670,29 @@ __global__ void __launch_bounds__(kScanThreads) k_compact(uint32_t* __restrict__
 // the context.  Group starts are marked at their first target's index for
 // the compaction.
 constexpr uint32_t kPackChunk = 2048;
+constexpr int kPackWindows = 4;  // windows of 32 targets whose counts are loaded together
+
+// Index of the first target whose particles start at or after particle p
+// (the targets lie in particle order), by one warp: each round probes 32
+// evenly spaced targets and keeps the stretch between the last probe before
+// p and the first one at or after it.
+__device__ __forceinline__ uint32_t first_target_at(const uint32_t* __restrict__ targets,
+                                                    const uint32_t* __restrict__ nbegin, uint32_t nt, uint32_t p,
+                                                    int lane) {
+  uint32_t lo = 0, hi = nt;  // the answer lies in [lo, hi]
+  while (hi - lo > 32u) {
+    const uint32_t step = (hi - lo + 31u) / 32u;
+    const uint32_t q = lo + (uint32_t)lane * step;
+    const bool before = q < hi && nbegin[targets[q]] < p;
+    const uint32_t m = (uint32_t)__popc(__ballot_sync(0xffffffffu, before));  // probes 0 .. m-1 lie before p
+    const uint32_t nlo = m ? lo + (m - 1u) * step + 1u : lo;
+    hi = min(hi, lo + m * step);
+    lo = nlo;
+  }
+  const uint32_t q = lo + (uint32_t)lane;
+  const bool before = q < hi && nbegin[targets[q]] < p;
+  return lo + (uint32_t)__popc(__ballot_sync(0xffffffffu, before));
+}
 
 __global__ void k_pack_groups(const uint32_t* __restrict__ chunks, const uint32_t* __restrict__ targets,
                               const uint32_t* __restrict__ nbegin, const uint32_t* __restrict__ ncount,
@@ -681,42 +704,42 @@ __global__ void k_pack_groups(const uint32_t* __restrict__ chunks, const uint32_
   for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < nchunks; c += gridDim.x * wpb) {
     const uint32_t cn = chunks[c];
     const uint32_t cb = nbegin[cn], ce = cb + ncount[cn];
-    // the chunk's first target: the first whose particles start at or after cb
-    uint32_t lo = 0, hi = nt;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (nbegin[targets[mid]] < cb) lo = mid + 1;
-      else hi = mid;
-    }
     uint32_t cnt = 0, k = 0;
-    bool first = true;
-    for (uint32_t t0 = lo;; t0 += 32) {
-      const uint32_t t = t0 + lane;
-      uint32_t n = 0xffffffffu;  // past the chunk
-      if (t < nt) {
-        const uint32_t tn = targets[t];
-        if (nbegin[tn] < ce) n = ncount[tn];
-      }
-      // the greedy packing, run alike by every lane over the 32 counts
-      uint32_t starts = 0;
-      bool end = false;
-      for (int i = 0; i < 32; ++i) {
-        const uint32_t ni = __shfl_sync(0xffffffffu, n, i);
-        if (ni == 0xffffffffu) {
-          end = true;
-          break;
+    bool first = true, end = false;
+    for (uint32_t t0 = first_target_at(targets, nbegin, nt, cb, lane); !end; t0 += 32u * kPackWindows) {
+      // the particle counts of the next windows' targets (past the chunk: ~0)
+      uint32_t n[kPackWindows];
+#pragma unroll
+      for (int w = 0; w < kPackWindows; ++w) {
+        const uint32_t t = t0 + 32u * w + (uint32_t)lane;
+        n[w] = 0xffffffffu;
+        if (t < nt) {
+          const uint32_t tn = targets[t];
+          if (nbegin[tn] < ce) n[w] = ncount[tn];
         }
-        if (first || cnt + ni > pack || k >= (uint32_t)kMaxTargets) {
-          starts |= 1u << i;
-          cnt = 0;
-          k = 0;
-          first = false;
-        }
-        cnt += ni;
-        ++k;
       }
-      if ((starts >> lane) & 1u) mark[t] = t;
-      if (end) break;
+#pragma unroll
+      for (int w = 0; w < kPackWindows; ++w) {
+        if (end) break;
+        // the greedy packing, run alike by every lane over the window's 32 counts
+        uint32_t starts = 0;
+        for (int i = 0; i < 32; ++i) {
+          const uint32_t ni = __shfl_sync(0xffffffffu, n[w], i);
+          if (ni == 0xffffffffu) {
+            end = true;
+            break;
+          }
+          if (first || cnt + ni > pack || k >= (uint32_t)kMaxTargets) {
+            starts |= 1u << i;
+            cnt = 0;
+            k = 0;
+            first = false;
+          }
+          cnt += ni;
+          ++k;
+        }
+        if ((starts >> lane) & 1u) mark[t0 + 32u * w + (uint32_t)lane] = t0 + 32u * w + (uint32_t)lane;
+      }
     }
   }
 }

@@ -268,6 +268,7 @@ int bhg_device_status(bhg_context* ctx, uint32_t* status);
 #define BHG_EXPORT_DOMAINS 5 /* double [systems][4]: centre xyz, half width */
 #define BHG_EXPORT_TARGETS 6 /* uint32 target node indices [targets] */
 #define BHG_EXPORT_ACCEL 7   /* double [n][3]: G*a of the last walk, output order */
+#define BHG_EXPORT_GROUPS 8  /* uint32 index (into the targets) of each walk group's first target [groups] */
 /* Copies one of the arrays above to host memory (blocks).  bytes must be at
  * least the array's size; *written receives the size. */
 int bhg_debug_export(bhg_context* ctx, int what, void* out, size_t bytes, size_t* written);

@@ -393,3 +393,62 @@ def test_unsoftened_system_among_softened_ones(precision):
         alone.step(bhg.Context.params(0.5, 0.0, 1.0, True, precision), 16, 256, 16, 0.01, 0.01)
         got = alone.download()
     assert got.tobytes() == out[at:at + len(systems[1])].tobytes()
+
+
+def _cut(g, lim):
+    """Topmost nodes holding at most lim particles, or leaves, depth first in
+    child order from each root (the target rule of bho_targets)."""
+    out = []
+    for r in np.flatnonzero(g["depth"] == 0):
+        st = [int(r)]
+        while st:
+            i = st.pop()
+            if g["leaf"][i] or g["count"][i] <= lim:
+                out.append(i)
+                continue
+            st.extend(int(g["first_child"][i]) + c for c in range(int(g["nchild"][i]) - 1, -1, -1))
+    return np.array(out, np.uint32)
+
+
+def _pack(g, targets, chunks, pack, max_targets=24):
+    """Walk groups: inside each packing chunk, consecutive targets packed
+    greedily while the group holds at most `pack` particles and max_targets
+    targets (a larger target is a group of its own); the index of each
+    group's first target."""
+    begin, count = g["begin"], g["count"]
+    tb = begin[targets]
+    starts = []
+    for c in chunks:
+        cb, ce = int(begin[c]), int(begin[c]) + int(count[c])
+        j = int(np.searchsorted(tb, cb, side="left"))
+        first, cnt, k = True, 0, 0
+        while j < len(targets) and tb[j] < ce:
+            n = int(count[targets[j]])
+            if first or cnt + n > pack or k >= max_targets:
+                starts.append(j)
+                first, cnt, k = False, 0, 0
+            cnt += n
+            k += 1
+            j += 1
+    return np.array(starts, np.uint32)
+
+
+@pytest.mark.parametrize("group", [1, 5, 32, 64])
+def test_walk_groups_follow_the_packing_rule(group):
+    """The walk groups of a three-system batch are the greedy packing of each
+    system's targets inside its packing chunks (nodes of at most 2,048
+    particles), whatever the walk-group cap."""
+    systems = [bhg.plummer(65536, 1)[0], bhg.plummer(3000, 7)[0], bhg.plummer(40000, 8)[0]]
+    fp = bhg.Context.params(0.5, 1e-4, 1.0, True, bhg.PRECISION_SPLIT)
+    with bhg.Context(device=0) as ctx:
+        ctx.set_walk_shape(group)
+        ctx.upload_systems(systems)
+        ctx.set_system_params(theta=np.full(3, 0.5), eps2=np.full(3, 1e-4), kick_dt=np.full(3, 0.01),
+                              drift_dt=np.full(3, 0.01))
+        ctx.step_systems(fp, 16, 256, 16)
+        g = ctx.tree()
+        targets = ctx.export(bhg.EXPORT_TARGETS)
+        groups = ctx.export(bhg.EXPORT_GROUPS)
+    assert np.array_equal(targets, _cut(g, 16))
+    want = _pack(g, targets, _cut(g, 2048), group)
+    assert len(groups) == len(want) and np.array_equal(groups, want)
