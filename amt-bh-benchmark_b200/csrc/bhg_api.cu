@@ -485,6 +485,9 @@ void enq_walk(bhg_context* c, bool want_accel) {
   a.gsum = reinterpret_cast<double*>(reinterpret_cast<char*>(c->list_buf) +
                                      c->list_warps * (walk_slot_bytes() - kGroupMax * 3 * sizeof(double) - sizeof(uint32_t)));
   a.gnl = reinterpret_cast<uint32_t*>(a.gsum + c->list_warps * kGroupMax * 3);
+  // list lengths "pending" (bytes 0xfe): the two-pass schedule's target jobs
+  // wait for their group's length
+  cudaMemsetAsync(a.gnl, 0xfe, c->list_warps * sizeof(uint32_t), c->stream);
   launch_walk(a, c->precision, c->quad != 0, c->mask, walk_launch_grid(c), c->stream);
   launch_eval_done(c->st, c->stream);
 }
@@ -1442,9 +1445,9 @@ int bhg_get_stats(bhg_context* c, bhg_stats* out, int reset) {
   // bounds + domain + keys + digit offsets; the sort passes; gather + roots +
   // one per level; the multipoles (one kernel, or one per level); mark +
   // compact of the targets, of the packing chunks, packing + compact of the
-  // walk groups; walk + its target pass + its completion count
+  // walk groups; the walk and its completion count
   out->kernels_per_eval = 4 + kSortPasses + (2 + kMortonDepth) + (c->n <= kMomentsOneLaunchMax ? 1 : kMortonDepth + 1) + 6 +
-                          3;
+                          2;
   if (reset) {
     for (double& t : c->tot_ms) t = 0.0;
     c->walks_timed = 0;

@@ -61,6 +61,9 @@ constexpr uint32_t kMaxRun = 255;
 static_assert(kMaxTargets <= kCountShift, "target masks and run lengths share a word");
 constexpr uint32_t kListCap = 4096;         // entries of one partial-source list (32 KB)
 constexpr uint32_t kNotShared = 0xffffffffu;  // a group whose list overflowed: its targets walk alone
+// a group's list length before its shared walk has finished (two-pass schedule;
+// the host fills the lengths with this byte pattern before every walk)
+constexpr uint32_t kListPending = 0xfefefefeu;
 // a walk that pops one node at a time holds at most 7 entries per level
 // below the one it pops from, plus the root
 static_assert(kStackCap >= 7 * kLevels + 1 + 8, "a one-at-a-time walk must fit the stack");
@@ -913,6 +916,74 @@ __device__ __forceinline__ GroupInfo group_info(const WalkArgs& a, uint32_t gi, 
   return g;
 }
 
+// The second pass of the two-pass schedule (see k_walk): one warp per target
+// of a group of more than one target, once its group's shared walk has
+// finished (its list length is no longer kListPending): the group's FP64 sums
+// for its particles, then its pass over the group's list (or, if the list
+// overflowed, its own walk from the root), then the kick/drift.  A job waits
+// only for a group whose walk a running warp has taken, so every wait ends;
+// a wait is still bounded (kStSpinLimit, the job skipped).
+template <class E, bool QUAD>
+__device__ __forceinline__ void target_jobs(E& ev, const WalkArgs& a, WarpSmem& S, uint32_t ngroups, uint32_t ntargets,
+                                            int lane, Queues& q, unsigned long long& n_pp, unsigned long long& n_pc) {
+  for (;;) {
+    uint32_t ti = 0;
+    if (lane == 0) ti = atomicAdd(&a.st->walk_next2, 1u);
+    ti = __shfl_sync(kFull, ti, 0);
+    if (ti >= ntargets) break;
+    // its group: the last whose first target is at or before ti
+    uint32_t gi = 0, hi = ngroups;
+    while (hi - gi > 1) {
+      const uint32_t mid = (gi + hi) >> 1;
+      if (a.groups[mid] <= ti) gi = mid;
+      else hi = mid;
+    }
+    const GroupInfo g = group_info(a, gi, ngroups, ntargets);
+    if (g.k == 1) continue;  // done whole in the first pass
+    uint32_t nlist = ld_volatile(a.gnl + gi);
+    for (int spins = 0; nlist == kListPending && spins < kSpinLimit; ++spins) {
+      __nanosleep(128);
+      nlist = ld_volatile(a.gnl + gi);
+    }
+    if (nlist == kListPending) {
+      if (lane == 0) atomicOr(&a.st->status, kStSpinLimit);
+      continue;
+    }
+    __threadfence();  // the group's sums and list after its length
+    const uint32_t tnode = a.targets[ti];
+    const uint32_t tb = a.nbegin[tnode], tn = a.ncount[tnode];  // tn <= kGroupMax: inside a group
+    const uint32_t root = a.sys[g.s].root;
+    const SysParam& sp = a.prm[g.s];
+    ev.set_system(sp.eps2, a.sys[g.s].hw);
+    double lo[3], hi3[3];
+    particle_box(a.pm, tb, tn, lane, lo, hi3);
+    ev.cx = 0.5 * (lo[0] + hi3[0]), ev.cy = 0.5 * (lo[1] + hi3[1]), ev.cz = 0.5 * (lo[2] + hi3[2]);
+    if (nlist == kNotShared) {
+      for (uint32_t i = lane; i < tn; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
+      __syncwarp();
+      int r = 0;
+      for (int attempt = 0; attempt < 2; ++attempt) {
+        ev.setup(lane, tb, (int)tn, S.acc);
+        r = target_walk(ev, a, S, root, lo, hi3, sp.theta2, attempt == 1, lane, q);
+        if (r == 0) break;
+      }
+      ev.finish();
+      add_counts(q, tn, QUAD, n_pp, n_pc);
+    } else {
+      const double* gs = a.gsum + (size_t)gi * (kGroupMax * 3) + 3 * (size_t)(tb - g.p0);
+      for (uint32_t i = lane; i < tn; i += 32) S.acc[i][0] = gs[3 * i], S.acc[i][1] = gs[3 * i + 1], S.acc[i][2] = gs[3 * i + 2];
+      __syncwarp();
+      if (nlist) {
+        ev.setup(lane, tb, (int)tn, S.acc);
+        target_pass(ev, a, S, a.wlist + (size_t)gi * kListCap, nlist, ti - g.t0, lane, q);
+        ev.finish();
+        add_counts(q, tn, QUAD, n_pp, n_pc);
+      }
+    }
+    kick_drift(a, sp, S.acc, tb, tn, lane);
+  }
+}
+
 // One warp per walk group (a run of targets, k_pack_groups).  A group of one
 // target larger than kGroupMax particles walks in batches of kGroupMax
 // targets.  Otherwise: the group's shared walk with every source all its
@@ -922,11 +993,12 @@ __device__ __forceinline__ GroupInfo group_info(const WalkArgs& a, uint32_t gi, 
 //
 // With few groups (n_groups <= a.nslots: about as many as warps, so the
 // largest group's targets would set the kernel's time) the work is cut in
-// two passes instead: this kernel runs the shared walks (and the groups of
-// one target whole) and leaves each group's FP64 sums and list in its own
-// slot; k_walk_targets then runs every target's pass as a job of its own.
-// Both schedules run the same passes and add each target's part onto the
-// group's sums the same way, so the results are the same bits.
+// two passes instead: the warps first take the shared walks (and the groups
+// of one target whole), each leaving its group's FP64 sums and list in the
+// group's slot, then take every target's pass as a job of its own, each
+// starting as soon as its group's walk is done (target_jobs).  Both
+// schedules run the same passes and add each target's part onto the group's
+// sums the same way, so the results are the same bits.
 template <class E, bool QUAD>
 __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1020,13 +1092,14 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
       ev.finish();
       add_counts(q, np, QUAD, n_pp, n_pc);
     }
-    if (split) {  // the targets' passes run in k_walk_targets
+    if (split) {  // the targets' passes run as jobs of their own (target_jobs)
       if (r == 0) {
         double* gs = a.gsum + (size_t)gi * (kGroupMax * 3);
         for (uint32_t i = lane; i < np; i += 32) gs[3 * i] = S.acc[i][0], gs[3 * i + 1] = S.acc[i][1], gs[3 * i + 2] = S.acc[i][2];
       }
-      if (lane == 0) a.gnl[gi] = r == 0 ? nlist : kNotShared;
+      __threadfence();  // the sums and the list before the length
       __syncwarp();
+      if (lane == 0) st_volatile(a.gnl + gi, r == 0 ? nlist : kNotShared);
       continue;
     }
     if (r == 0) {
@@ -1049,74 +1122,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk(WalkArgs a) {
     }
     kick_drift(a, sp, S.acc, p0, np, lane);
   }
-  if (lane == 0) {
-    atomicAdd(&a.st->pp, n_pp);
-    atomicAdd(&a.st->pc, n_pc);
-  }
-}
-
-// The second pass of the two-pass schedule (see k_walk): one warp per target
-// of a group of more than one target: the group's FP64 sums for its
-// particles, then its pass over the group's list (or, if the list
-// overflowed, its own walk from the root), then the kick/drift.
-template <class E, bool QUAD>
-__global__ void __launch_bounds__(kWalkThreads, 4) k_walk_targets(WalkArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  WarpSmem& S = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  if (a.st->status & (kStNonFinite | kStNodeOverflow | kStSpinLimit)) return;
-  const uint32_t ngroups = a.st->n_groups, ntargets = a.st->n_targets;
-  if (ngroups > a.nslots) return;  // k_walk ran the one-pass schedule
-  unsigned long long n_pp = 0, n_pc = 0;
-  E ev(a, S.stage, lane);
-  Queues q;
-  for (;;) {
-    uint32_t ti = 0;
-    if (lane == 0) ti = atomicAdd(&a.st->walk_next2, 1u);
-    ti = __shfl_sync(kFull, ti, 0);
-    if (ti >= ntargets) break;
-    // its group: the last whose first target is at or before ti
-    uint32_t gi = 0, hi = ngroups;
-    while (hi - gi > 1) {
-      const uint32_t mid = (gi + hi) >> 1;
-      if (a.groups[mid] <= ti) gi = mid;
-      else hi = mid;
-    }
-    const GroupInfo g = group_info(a, gi, ngroups, ntargets);
-    if (g.k == 1) continue;  // done whole in the first pass
-    const uint32_t tnode = a.targets[ti];
-    const uint32_t tb = a.nbegin[tnode], tn = a.ncount[tnode];  // tn <= kGroupMax: inside a group
-    const uint32_t root = a.sys[g.s].root;
-    const SysParam& sp = a.prm[g.s];
-    ev.set_system(sp.eps2, a.sys[g.s].hw);
-    double lo[3], hi3[3];
-    particle_box(a.pm, tb, tn, lane, lo, hi3);
-    ev.cx = 0.5 * (lo[0] + hi3[0]), ev.cy = 0.5 * (lo[1] + hi3[1]), ev.cz = 0.5 * (lo[2] + hi3[2]);
-    const uint32_t nlist = a.gnl[gi];
-    if (nlist == kNotShared) {
-      for (uint32_t i = lane; i < tn; i += 32) S.acc[i][0] = S.acc[i][1] = S.acc[i][2] = 0.0;
-      __syncwarp();
-      int r = 0;
-      for (int attempt = 0; attempt < 2; ++attempt) {
-        ev.setup(lane, tb, (int)tn, S.acc);
-        r = target_walk(ev, a, S, root, lo, hi3, sp.theta2, attempt == 1, lane, q);
-        if (r == 0) break;
-      }
-      ev.finish();
-      add_counts(q, tn, QUAD, n_pp, n_pc);
-    } else {
-      const double* gs = a.gsum + (size_t)gi * (kGroupMax * 3) + 3 * (size_t)(tb - g.p0);
-      for (uint32_t i = lane; i < tn; i += 32) S.acc[i][0] = gs[3 * i], S.acc[i][1] = gs[3 * i + 1], S.acc[i][2] = gs[3 * i + 2];
-      __syncwarp();
-      if (nlist) {
-        ev.setup(lane, tb, (int)tn, S.acc);
-        target_pass(ev, a, S, a.wlist + (size_t)gi * kListCap, nlist, ti - g.t0, lane, q);
-        ev.finish();
-        add_counts(q, tn, QUAD, n_pp, n_pc);
-      }
-    }
-    kick_drift(a, sp, S.acc, tb, tn, lane);
-  }
+  if (two_pass) target_jobs<E, QUAD>(ev, a, S, ngroups, ntargets, lane, q, n_pp, n_pc);
   if (lane == 0) {
     atomicAdd(&a.st->pp, n_pp);
     atomicAdd(&a.st->pc, n_pc);
@@ -1126,7 +1132,6 @@ __global__ void __launch_bounds__(kWalkThreads, 4) k_walk_targets(WalkArgs a) {
 template <class E, bool QUAD>
 static void launch_one(const WalkArgs& a, int grid, cudaStream_t s) {
   k_walk<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
-  k_walk_targets<E, QUAD><<<grid, kWalkThreads, kWalkSmem, s>>>(a);
 }
 
 void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int grid, cudaStream_t s) {
@@ -1142,7 +1147,6 @@ void launch_walk(const WalkArgs& a, int precision, bool quad, bool mask, int gri
 template <class E, bool QUAD>
 static int occ() {
   cudaFuncSetAttribute(k_walk<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
-  cudaFuncSetAttribute(k_walk_targets<E, QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem);
   int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk<E, QUAD>, kWalkThreads, kWalkSmem);
   return b > 0 ? b : 1;
