@@ -439,7 +439,8 @@ void enq_sort(bhg_context* c) {
 void enq_tree(bhg_context* c) {
   // kSortPasses is even: sorted keys and the permutation are back in [0]
   launch_gather(c->part, c->vals[0], (uint32_t)c->n, c->staged, c->pm, c->sms, c->stream);
-  launch_topology(c->sys, c->nsys, c->nd, c->keys[0], c->max_leaf, c->level_lb, c->st, c->sms, c->stream);
+  launch_topology(c->sys, c->nsys, c->nd, c->keys[0], c->max_leaf, (uint32_t)c->n, c->level_lb, c->st, c->sms,
+                  c->stream);
 }
 
 // Multipoles in one launch up to this many particles (the per-level launches

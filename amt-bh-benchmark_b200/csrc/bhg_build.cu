@@ -7,6 +7,7 @@
 // (explicit round-to-nearest intrinsics, no contraction).
 #include "bhg_kernels.h"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace bhg {
@@ -933,11 +934,29 @@ void launch_gather(const Particle* p, const uint32_t* perm, uint32_t n, Particle
   k_gather<<<blocks, 256, 0, s>>>(p, perm, n, staged, pm);
 }
 
-void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_t* keys, unsigned max_leaf,
+// Blocks for a grid that takes `units` work items `per_block` at a time, at
+// most `cap` blocks (the rest of a larger grid would find no work).
+static int grid_for(uint64_t units, uint64_t per_block, int cap) {
+  const uint64_t b = (units + per_block - 1) / per_block;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)cap));
+}
+
+// The nodes of level d-1 (the parents k_level reads) are at most 8^(d-1)
+// per root, at most n, and at most 8 per interior node of the level above
+// (an interior node holds more than max_leaf particles: at most
+// n / (max_leaf + 1) of them per level), so the upper levels launch only the
+// blocks that can find a tile.
+void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_t* keys, unsigned max_leaf, uint32_t n,
                      uint32_t* lookback, DevState* st, int sms, cudaStream_t s) {
   k_roots<<<(nsys + 127) / 128, 128, 0, s>>>(sys, nsys, nd, max_leaf, st);
-  for (int d = 1; d <= kMortonDepth; ++d)
-    k_level<<<sms * kLevelBlocksPerSm, kLevelThreads, 0, s>>>(d, nd, keys, max_leaf, lookback, st);
+  const uint64_t below = std::min<uint64_t>(n, 8 * ((uint64_t)n / ((uint64_t)max_leaf + 1) + (uint64_t)nsys));
+  uint64_t width = (uint64_t)nsys;  // 8^(d-1) per root
+  for (int d = 1; d <= kMortonDepth; ++d) {
+    const uint64_t parents = std::min(width, below);
+    k_level<<<grid_for(parents, kLevelParents, sms * kLevelBlocksPerSm), kLevelThreads, 0, s>>>(d, nd, keys, max_leaf,
+                                                                                               lookback, st);
+    width = std::min<uint64_t>(width * 8, 1ull << 40);
+  }
 }
 
 // Grids of the cut kernels (tiles and nodes taken by grid stride or by a
@@ -946,21 +965,22 @@ void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_
 void launch_targets(const Nodes& nd, uint32_t lim, uint32_t pack, uint32_t n, uint32_t* mark, uint32_t* targets,
                     uint32_t* chunks, uint32_t* groups, uint32_t* lookback, DevState* st, int sms, cudaStream_t s) {
   const uint32_t ntiles = (n + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
-  k_mark_cut<<<sms * 16, 256, 0, s>>>(nd, lim, st, mark);
-  k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, targets, lookback, &st->scan_tiles, &st->n_targets, st);
-  k_mark_cut<<<sms * 16, 256, 0, s>>>(nd, kPackChunk, st, mark);
-  k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, chunks, lookback + (ntiles + 8), &st->chunk_tiles,
-                                             &st->n_chunks, st);
+  const int gmark = grid_for(nd.cap, 256, sms * 16), gscan = grid_for(ntiles, 1, sms * 8);
+  k_mark_cut<<<gmark, 256, 0, s>>>(nd, lim, st, mark);
+  k_compact<<<gscan, kScanThreads, 0, s>>>(mark, n, targets, lookback, &st->scan_tiles, &st->n_targets, st);
+  k_mark_cut<<<gmark, 256, 0, s>>>(nd, kPackChunk, st, mark);
+  k_compact<<<gscan, kScanThreads, 0, s>>>(mark, n, chunks, lookback + (ntiles + 8), &st->chunk_tiles, &st->n_chunks,
+                                           st);
   k_pack_groups<<<sms * 4, 256, 0, s>>>(chunks, targets, nd.begin, nd.count, pack, st, mark);
-  k_compact<<<sms * 8, kScanThreads, 0, s>>>(mark, n, groups, lookback + 2 * (ntiles + 8), &st->group_tiles,
-                                             &st->n_groups, st);
+  k_compact<<<gscan, kScanThreads, 0, s>>>(mark, n, groups, lookback + 2 * (ntiles + 8), &st->group_tiles,
+                                           &st->n_groups, st);
 }
 
 // Per-level multipoles at 16 blocks of 128 per SM: 0.233 ms at 4M, 0.270
 // with 4.
 void launch_moments(const Nodes& nd, const double4* pm, const DevState* st, int sms, bool one_launch, cudaStream_t s) {
   if (one_launch) {
-    k_moments_up<<<sms * 4, 128, 0, s>>>(nd, pm, st);
+    k_moments_up<<<grid_for(nd.cap, 128, sms * 4), 128, 0, s>>>(nd, pm, st);
   } else {
     for (int d = kMortonDepth; d >= 0; --d) k_moments<<<sms * 16, 128, 0, s>>>(d, nd, pm, st);
   }

@@ -20,7 +20,7 @@ void launch_sort_pass(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, 
                       DevState* st, cudaStream_t s);
 void launch_gather(const Particle* p, const uint32_t* perm, uint32_t n, Particle* staged, double4* pm, int sms,
                    cudaStream_t s);
-void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_t* keys, unsigned max_leaf,
+void launch_topology(const SysDev* sys, int nsys, const Nodes& nd, const uint64_t* keys, unsigned max_leaf, uint32_t n,
                      uint32_t* lookback, DevState* st, int sms, cudaStream_t s);
 // Walk targets: the topmost nodes that are leaves or hold at most `lim`
 // particles.  The reference visits each group root - the topmost nodes with
