@@ -945,6 +945,7 @@ __device__ __forceinline__ void target_jobs(E& ev, const WalkArgs& a, WarpSmem& 
       __nanosleep(128);
       nlist = ld_volatile(a.gnl + gi);
     }
+    nlist = __shfl_sync(kFull, nlist, 0);  // one value for the warp
     if (nlist == kListPending) {
       if (lane == 0) atomicOr(&a.st->status, kStSpinLimit);
       continue;
