@@ -262,21 +262,8 @@ constexpr size_t sort_smem() {
   return (size_t)NT * ITEMS * 12 + (size_t)(NT / 32) * kDigits * 4 + kDigits * 4 + 4 * (NT / 32 + 2);
 }
 
-// The lanes of the warp whose 8-bit digit equals this lane's, among the
-// lanes with ok set (the result of a lane without ok is not used): one ballot
-// per digit bit, which the SM issues faster than a match instruction.
-__device__ __forceinline__ uint32_t match_digit(uint32_t dg, bool ok) {
-  uint32_t m = __ballot_sync(0xffffffffu, ok);
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const bool bit = (dg >> b) & 1u;
-    const uint32_t on = __ballot_sync(0xffffffffu, bit);
-    m &= bit ? on : ~on;
-  }
-  return m;
-}
-
-// match_digit with every lane's key in the tile
+// The lanes of the warp whose 8-bit digit equals this lane's: one ballot per
+// digit bit, which the SM issues faster than a match instruction.
 __device__ __forceinline__ uint32_t match_digit_all(uint32_t dg) {
   uint32_t m = 0xffffffffu;
 #pragma unroll
@@ -286,6 +273,12 @@ __device__ __forceinline__ uint32_t match_digit_all(uint32_t dg) {
     m &= bit ? on : ~on;
   }
   return m;
+}
+
+// The same among the lanes with ok set (the result of a lane without ok is
+// not used).
+__device__ __forceinline__ uint32_t match_digit(uint32_t dg, bool ok) {
+  return __ballot_sync(0xffffffffu, ok) & match_digit_all(dg);
 }
 
 // A pass's tile: keys (and, after the first pass, values) into registers,
