@@ -60,6 +60,12 @@ std::vector<Particle> step_particles(std::vector<Particle> particles, const Forc
   static_assert(std::is_trivially_copyable_v<Particle>, "Particle must be trivially copyable");
   if (group_size == 0)
     throw std::invalid_argument("group_size 0 selects the reference's per-node pass; the GPU path is the grouped one");
+  if (particles.empty()) {
+    // the reference builds an empty tree (flat_build_ttg.h:215) and walks
+    // nothing: the same empty vector comes back
+    if (timing) timing->tree_build_ms = timing->traversal_ms = timing->exchange_ms = 0.0;
+    return particles;
+  }
   Workspace* ws = workspace;
   std::unique_ptr<Workspace> own;
   if (!ws) {

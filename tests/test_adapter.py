@@ -73,3 +73,17 @@ def test_adapter_schedule_matches_oracle(tmp_path, oracle, precision, pos_tol):
     o, r = out[np.argsort(out["id"])], ref[np.argsort(ref["id"])]
     assert np.array_equal(o["id"], r["id"])
     assert np.max(np.abs(o["pos"] - r["pos"])) < pos_tol
+
+
+@pytest.mark.gpu
+def test_adapter_empty_input_comes_back_empty(tmp_path):
+    """An empty particle vector: the reference builds an empty tree and walks
+    nothing (flat_build_ttg.h:215); the drop-in returns the empty vector."""
+    exe = str(tmp_path / "adapter")
+    compile_adapter(exe)
+    src, dst = tmp_path / "in.bin", tmp_path / "out.bin"
+    src.write_bytes(b"")
+    r = subprocess.run([exe, str(src), str(dst), "0.5", "0.01", repr(1 / 128), "2", "0"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert dst.read_bytes() == b""
