@@ -11,6 +11,9 @@ the global norm of test_bh_vs_bruteforce.cc:30-40.
   merger (seed 4, theta 0.6, eps 0.002): the build bit for bit against the
   oracle, and the split forces of 4,096 sampled walk targets against the
   oracle's walk of just those targets (bh_oracle.c bho_walk takes a target list).
+* The 512-system ensemble (seed 3, eps 0.01) evaluated as one batch: the
+  split forces of sampled targets of three of its systems against the
+  oracle's walk of each system alone.
 
 The oracle (oracle/bh_oracle.c) is pinned to the reference compiled from its
 own sources (tests/test_oracle_pin.py)."""
@@ -157,3 +160,34 @@ def test_large_build_bit_exact_and_sampled_forces(oracle, name):
     s = _rel_stats(acc[rows], racc[rows])
     print(f"{name}: {len(sample)} targets, {len(rows)} particles: {s}")
     assert s["rms"] <= SPLIT_TOL and s["p99"] <= SPLIT_TOL and s["global"] <= SPLIT_TOL, s
+
+
+# ------------------------------------------------------------------ 512-system ensemble
+
+
+def test_ensemble512_batched_forces_match_oracle(oracle):
+    """The 512-system ensemble (N log-uniform in [1,024, 262,144], seed 3,
+    eps 0.01, theta 0.5, leaf/target 16) evaluated as one segmented batch in
+    split precision: for the smallest, a middle and the largest system, the
+    forces of sampled walk targets against the oracle's walk of that system
+    alone (per-particle rms and p99 within the split tolerance)."""
+    systems = bhg.ensemble(512, 3)
+    ns = np.array([len(p) for p in systems])
+    begins = np.concatenate([[0], np.cumsum(ns)[:-1]])
+    eps2, theta = 0.01 ** 2, 0.5
+    with bhg.Context(device=0) as ctx:
+        ctx.upload_systems(systems)
+        ctx.build_tree(16, 256)
+        ctx.compute_multipoles()
+        acc = ctx.walk_forces(bhg.Context.params(theta, eps2, 1.0, True, bhg.PRECISION_SPLIT), 16)
+    order = np.argsort(ns)
+    for s in (int(order[0]), int(order[len(order) // 2]), int(order[-1])):
+        dom, sk, perm, mp, t = _oracle_build(oracle, systems[s], 16)
+        tg = oracle.targets(t, 16, 256)
+        pick = tg if len(tg) <= 2048 else tg[np.sort(np.random.default_rng(s).choice(len(tg), 2048, replace=False))]
+        racc, _ = oracle.walk(t, pick, soa(mp), [Params(theta, eps2, 1.0, 1)] * len(pick))
+        rows = np.concatenate([np.arange(t["begin"][x], t["begin"][x] + t["count"][x]) for x in pick])
+        got = acc[begins[s]:begins[s] + ns[s]][rows]
+        st = _rel_stats(got, racc[rows])
+        print(f"ensemble system {s} (N={ns[s]}): {len(pick)} targets: {st}")
+        assert st["rms"] <= SPLIT_TOL and st["p99"] <= SPLIT_TOL and st["global"] <= SPLIT_TOL, st
