@@ -98,7 +98,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="ensemble: skip the one-at-a-time FP64 path")
     ap.add_argument("--walk-group", type=int, default=0,
                     help="single systems: walk-group particle cap (0 = the library's default)")
-    ap.add_argument("--no-north-star", action="store_true",
+    ap.add_argument("--no-gates", action="store_true",
                     help="plummer-4m: skip the ensemble and serving gates run after the main measurement")
     ap.add_argument("--serve-budget-gb", type=float, default=None, help="serve: HBM admission budget")
     ap.add_argument("--serve-wall", type=float, default=None, help="serve: wall-clock window in seconds")
@@ -577,8 +577,8 @@ def bench_single(args, w, rig, bhg, fp32_peak, peaks):
 
 
 def bench_ensemble(args, w, rig, bhg, fp32_peak, peaks, quick=False):
-    """quick: the north-star check inside the default run - fewer timed
-    steps, no pipelined end-to-end leg, no CPU baseline."""
+    """quick: the gate check inside the default run - fewer timed steps, no
+    pipelined end-to-end leg, no CPU baseline."""
     from bhg import autotune
 
     if quick:
@@ -802,7 +802,7 @@ def bench_csv(args, w, rig, bhg, peaks):
 def bench_serve(args, w, rig, bhg, fp32_peak, peaks, quick=False):
     """The request loop in real time over the Poisson stream, for a bounded
     wall window; value = particle-steps completed / wall time.  quick: the
-    north-star check inside the default run - a 30 s window, no CPU baseline."""
+    gate check inside the default run - a 30 s window, no CPU baseline."""
     from bhg import serve
 
     w = dict(w)
@@ -906,7 +906,7 @@ def bench_serve(args, w, rig, bhg, fp32_peak, peaks, quick=False):
     return out
 
 
-def north_star_block(args, rig, bhg, fp32_peak, peaks):
+def gates_block(args, rig, bhg, fp32_peak, peaks):
     """The two throughput gates of the batched and served paths, measured in
     the default run (each with its own clock record):
 
@@ -961,8 +961,8 @@ def main():
         dtype = "f32+f64" if args.precision == "split" else "f64"
     # the gates are single-GPU ones: not repeated on every replica of a
     # multi-GPU run
-    if w["kind"] == "single" and args.workload == "plummer-4m" and not args.no_north_star and rig.world == 1:
-        res["north_star"] = north_star_block(args, rig, bhg, fp32_peak, peaks)
+    if w["kind"] == "single" and args.workload == "plummer-4m" and not args.no_gates and rig.world == 1:
+        res["gates"] = gates_block(args, rig, bhg, fp32_peak, peaks)
     if rig.rank == 0:
         cfg = workload_config(args.workload, w, rig.world)
         metric, unit = (METRIC, "particle-steps/s") if w["kind"] != "csv" else ("csv-ingest particles/s", "particles/s")
