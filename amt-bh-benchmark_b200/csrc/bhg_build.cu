@@ -479,6 +479,27 @@ constexpr int kLevelParents = kLevelThreads / 8;
 // phase at 4M takes 0.97 ms with 4, 0.74 with 8, 0.75 with 16
 constexpr int kLevelBlocksPerSm = 8;
 
+// The first index in [lo, hi) whose key is >= thr (hi if none; keys sorted),
+// by an 8-way search: each round loads 7 evenly spaced keys at once and keeps
+// the stretch between the last one below thr and the first one at or above,
+// so a parent of 65,536 particles takes 6 dependent rounds instead of 16.
+__device__ __forceinline__ uint32_t first_at_least(const uint64_t* __restrict__ keys, uint32_t lo, uint32_t hi,
+                                                   uint64_t thr) {
+  while (hi - lo > 8u) {
+    const uint32_t step = (hi - lo) >> 3;
+    uint32_t m = 0;  // probes lo + j * step (j = 1..7) below thr: a prefix, the keys being sorted
+#pragma unroll
+    for (uint32_t j = 1; j <= 7; ++j) m += keys[lo + j * step] < thr ? 1u : 0u;
+    const uint32_t nlo = m ? lo + m * step + 1u : lo;
+    hi = m < 7u ? lo + (m + 1u) * step : hi;
+    lo = nlo;
+  }
+  uint32_t m = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < 8u; ++j) m += (lo + j < hi && keys[lo + j] < thr) ? 1u : 0u;
+  return lo + m;
+}
+
 __global__ void __launch_bounds__(kLevelThreads) k_level(int depth, Nodes nd, const uint64_t* __restrict__ keys,
                                                          unsigned max_leaf, uint32_t* __restrict__ lookback_all,
                                                          DevState* st) {
@@ -514,13 +535,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_level(int depth, Nodes nd, co
     if (split && oct > 0) {
       const uint64_t cell = 1ull << (csh + 3);  // parent's cell size in keys
       const uint64_t thr = (keys[b] & ~(cell - 1)) | ((uint64_t)oct << csh);
-      uint32_t lo = b, hi = b + c;
-      while (lo < hi) {
-        uint32_t mid = lo + ((hi - lo) >> 1);
-        if (keys[mid] < thr) lo = mid + 1;
-        else hi = mid;
-      }
-      start = lo;
+      start = first_at_least(keys, b, b + c, thr);
     }
     uint32_t next = __shfl_down_sync(0xffffffffu, start, 1);
     if (oct == 7) next = b + c;
